@@ -1,0 +1,410 @@
+#!/usr/bin/env python
+"""Benchmark: diffusion3d 7-point stencil, 512^3 FP32, 200 steps per step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One bench "step" is one RunKernel(200) of a 512^3 FP32 grid (the reference's
+workload unit; 2.68e10 point-updates).  `value` is whole-job Gpoint-updates/s
+with the field resident in HBM; `e2e` is the same metric through the
+RunKernel-style C-ABI call (d3d_run_host) with pinned host buffers, so the
+512 MiB host->device and device->host copies are inside its timed region.
+
+N > 1 (torchrun, one rank per GPU): every rank advances its own 512^3 grid
+(independent grids shard with no data-path collective: weak scaling); the
+time is the max over ranks.
+
+--impl reference times the reference's own Diffusion3DOpenMP::RunKernel
+(oracle/_ref, compiled from the reference sources; the C restatement in
+oracle/ when that is absent) on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_SIDE = 512
+COUNT = 200
+METRIC = "Gpoint-updates/s (512^3 FP32, 200 steps per RunKernel)"
+UNIT = "Gpt-updates/s"
+BYTES_PER_UPDATE = 8  # FP32: one 4-byte read + one 4-byte write per point
+PEAK_FALLBACK_GBS = 6650.0
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def measured_peak_gbs():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return PEAK_FALLBACK_GBS, "fallback"
+
+
+def profile_traffic(name):
+    """dram bytes per launch recorded in a committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", name)
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled while the timed work runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu),
+                 "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"),
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi"]}
+        time.sleep(0.2)
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        sm, smax, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        loaded = [s for s in sm if smax and s > 0.5 * smax] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": smax, "samples": len(sm),
+                "power_w_max": max(power) if power else None,
+                "reasons": sorted(reasons)}
+
+
+def cpu_reference_leg(n_side, steps_hint=None, budget_s=12.0):
+    """Times the reference's own Diffusion3DOpenMP::RunKernel on the host
+    (oracle/_ref), else the oracle port, on a bounded sample of the 512^3
+    workload.  Returns a cpu_baseline dict."""
+    import oracle as O
+    threads = os.cpu_count() or 1
+    kind = "reference" if O.ref_available() else "port"
+    n = n_side
+
+    def timed(count):
+        if kind == "reference":
+            t0 = time.perf_counter()
+            O.ref_run(n, n, n, count)
+            # ref_run includes the reference's InitializeBenchmark
+            # (host Initialize over 512^3); time it separately and remove.
+            return time.perf_counter() - t0
+        c, _ = O.params(n, n, n)
+        f = O.initialize(n, n, n)
+        t0 = time.perf_counter()
+        O.run(f, c, count)
+        return time.perf_counter() - t0
+
+    O.set_threads(threads)
+    t0 = timed(0)  # setup cost only (allocation + Initialize)
+    t2 = timed(2) - t0
+    per_step = max(t2 / 2, 1e-3)
+    steps = steps_hint or int(max(2, min(COUNT, budget_s / per_step)))
+    t = timed(steps) - t0
+    rate = n ** 3 * steps / t / 1e9
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": "%d^3 FP32, %d steps of Diffusion3DOpenMP::RunKernel "
+                      "(%s), %.2f s, setup excluded" % (
+                          n, steps, "oracle/_ref" if kind == "reference"
+                          else "oracle port", t)}
+
+
+def run_reference_arm(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    import oracle as O
+    if not os.path.exists(O.LIB_PATH) or (
+            not O.ref_available() and os.path.isdir(O.REF_SRC)):
+        O.build()
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    kind = "reference" if O.ref_available() else "port"
+    n = N_SIDE
+    sample_steps = 10  # bounded sample of the 200-step RunKernel per step
+
+    def one():
+        t0 = time.perf_counter()
+        if kind == "reference":
+            O.ref_run(n, n, n, 0)
+            t_setup = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            O.ref_run(n, n, n, sample_steps)
+            return time.perf_counter() - t0 - t_setup
+        c, _ = O.params(n, n, n)
+        f = O.initialize(n, n, n)
+        t0 = time.perf_counter()
+        O.run(f, c, sample_steps)
+        return time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        one()
+    times = [one() for _ in range(args.steps)]
+    total = sum(times)
+    value = n ** 3 * sample_steps * args.steps / total / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps * COUNT / sample_steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (reference Initialize, t=0)",
+        "config": {"workload": "diffusion3d 512^3 FP32, 200 steps per "
+                   "RunKernel; each timed step a %d-step sample" % sample_steps,
+                   "grid": [n, n, n], "count": COUNT, "l2": "input 512 MiB > L2"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                         "kind": kind,
+                         "sample": "%d^3, %d of the 200 steps per timed step, "
+                                   "Diffusion3DOpenMP::RunKernel, %d threads"
+                                   % (n, sample_steps, threads)},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args):
+    import torch
+    import benchmarks_b200 as B
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    n = N_SIDE
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    plan = B.Plan(n, n, n, B.F32, B.KERNEL_AUTO)
+    coeff = plan.reference_coefficients()
+    _, geom = B.coefficients(n, n, n, B.F32)
+
+    # Config: analytic sinusoid at t=0 plus seeded U[0, 1e-3) noise.
+    f1 = plan.empty()
+    f2 = plan.empty()
+    plan.analytic(f1, 0.0)
+    gen = torch.Generator(device=dev).manual_seed(0xD1FF + rank)
+    f1.add_(torch.rand(f1.shape, device=dev, generator=gen) * 1e-3)
+    init = f1.clone()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def run_steps(p, a, b, k):
+        for _ in range(k):
+            a, b = p.run(a, b, COUNT, coeff, stream)
+        return a, b
+
+    # --- headline: plain TMA z-march kernel ---------------------------
+    a, b = run_steps(plan, f1, f2, args.warmup)
+    try:
+        gpu_id = "GPU-%s" % torch.cuda.get_device_properties(local).uuid
+    except Exception:
+        gpu_id = str(local)
+    sampler = ClockSampler(gpu_id)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = B.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    a, b = run_steps(plan, a, b, args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    launches = B.launch_count() - launches0
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms)
+    updates = float(n) ** 3 * COUNT * args.steps
+    value = updates * world / (ms_max / 1e3) / 1e9
+    per_launch_s = ms / 1e3 / (COUNT * args.steps)
+    peak, peak_kind = measured_peak_gbs()
+    achieved = BYTES_PER_UPDATE * n ** 3 / per_launch_s / 1e9
+    traffic = profile_traffic("step_tma_512cube_f32.md")
+    info = plan.info()
+
+    # --- side measurements (not the headline) --------------------------
+    def rate_of(p, a_, b_, steps):
+        a_, b_ = run_steps(p, a_, b_, 1)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        a_, b_ = run_steps(p, a_, b_, steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        return float(n) ** 3 * COUNT * steps / t / 1e9, p.info()
+
+    side = {}
+    for k in (2, 3, 4):
+        ptb = B.Plan(n, n, n, B.F32, B.KERNEL_TB, k)
+        r, inf = rate_of(ptb, a, b, 3)
+        side["tb%d" % k] = {
+            "value": r, "unit": UNIT,
+            "effective_hbm_frac": r * 1e9 * BYTES_PER_UPDATE / (peak * 1e9),
+            "grid": inf["grid"], "smem": inf["smem"]}
+        ptb.close()
+
+    # --- correctness report: FP32 vs FP64 vs analytic, FP64 norms -------
+    plan64 = B.Plan(n, n, n, B.F64, B.KERNEL_AUTO)
+    c64 = plan64.reference_coefficients()
+    g1 = init.double()
+    g2 = torch.empty_like(g1)
+    r64, o64 = plan64.run(g1, g2, COUNT, c64, stream)
+    del o64
+    x1 = init.clone()
+    x2 = torch.empty_like(x1)
+    r32, o32 = plan.run(x1, x2, COUNT, coeff, stream)
+    del o32
+    ana = torch.empty_like(r64)
+    t_final = float(np.float32(COUNT) * geom[7])  # count * dt_, as the reference
+    plan64.analytic(ana, t_final, stream)
+    def norms(v):
+        return {"rms": v[0], "max_abs": v[1], "max_rel": v[2]}
+    report = {
+        "fp32_vs_fp64": norms(plan.compare(r32, r64, stream)),
+        "fp32_vs_analytic": norms(plan.compare(r32, ana, stream)),
+        "fp64_vs_analytic": norms(plan.compare(r64, ana, stream)),
+        "steps": COUNT, "input": "analytic(t=0) + U[0,1e-3) noise",
+    }
+    # FP64 throughput of the same workload (16 B per update).
+    r64_rate, _ = rate_of(plan64, g1, g2, 2)
+    side["fp64"] = {"value": r64_rate, "unit": UNIT,
+                    "hbm_frac": r64_rate * 16 / peak}
+    del g1, g2, r64, ana, x1, x2, r32, init
+    plan64.close()
+    torch.cuda.synchronize()
+
+    # --- e2e: RunKernel-style call with pinned host buffers -------------
+    host = B.pinned_empty((n, n, n), np.float32)
+    host[...] = 0
+    torch.cuda.synchronize()
+    for _ in range(1):
+        plan.run_host(host, a, b, COUNT, coeff, stream)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps // 2)):
+        plan.run_host(host, a, b, COUNT, coeff, stream)
+    t_e2e = time.perf_counter() - t0
+    e2e_steps = max(1, args.steps // 2)
+    t_e2e = max_over_ranks(t_e2e)
+    e2e = {"value": float(n) ** 3 * COUNT * e2e_steps * world / t_e2e / 1e9,
+           "unit": UNIT, "h2d_bytes_per_step": n ** 3 * 4,
+           "d2h_bytes_per_step": n ** 3 * 4}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: analytic sinusoid + seeded U[0,1e-3) noise",
+        "config": {"workload": "diffusion3d 512^3 FP32, 200 steps per "
+                   "RunKernel (plain TMA z-march kernel)",
+                   "grid": [n, n, n], "count": COUNT,
+                   "l2": "inputs larger than L2 (512 MiB per buffer)",
+                   "parallelism": "independent grid per GPU" if world > 1
+                   else "single GPU", "kernel": info},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind,
+                     "traffic": traffic,
+                     "algorithmic_bytes_per_launch": BYTES_PER_UPDATE * n ** 3},
+        "clocks": clocks,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "correctness": report,
+        "side": side,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_reference_leg(n)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true",
+                    help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,273 @@
+"""diffusion3d on B200: Python bindings over the C ABI of libd3d_b200.so.
+
+The product is the CUDA library behind ``include/d3d_b200.h``; this module
+binds it with ctypes so that tests, the benchmark and Python callers drive
+exactly the entry points a C/C++ caller (the ``Diffusion3DB200`` plugin)
+uses.  PyTorch is used only for device memory and streams.
+
+There is no CPU fallback: if the library is missing or no CUDA device is
+present, the compute entry points raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+LIB_PATH = os.path.join(PKG, "libd3d_b200.so")
+HEADER = os.path.join(ROOT, "include", "d3d_b200.h")
+
+D3D_OK = 0
+D3D_E_INVALID, D3D_E_CUDA, D3D_E_OOM = -1, -2, -3
+D3D_E_TIMEOUT, D3D_E_UNSUPPORTED, D3D_E_BUSY = -4, -5, -6
+F32, F64 = 0, 1
+KERNEL_AUTO, KERNEL_GENERIC, KERNEL_TMA, KERNEL_TB = 0, 1, 2, 3
+NUM_TILE_VARIANTS = 5
+
+_vp = ctypes.c_void_p
+_vpp = ctypes.POINTER(ctypes.c_void_p)
+_i = ctypes.c_int
+_sz = ctypes.c_size_t
+_dp = ctypes.POINTER(ctypes.c_double)
+
+_SIGNATURES = {
+    "d3d_version": ([], ctypes.c_char_p),
+    "d3d_last_error": ([], ctypes.c_char_p),
+    "d3d_launch_count": ([], ctypes.c_ulonglong),
+    "d3d_coefficients": ([_i, _i, _i, _i, _vp, _vp], _i),
+    "d3d_plan_create": ([_i, _i, _i, _i, _i, _i, _vpp], _i),
+    "d3d_plan_set_tile": ([_vp, _i, _i], _i),
+    "d3d_plan_destroy": ([_vp], _i),
+    "d3d_plan_info": ([_vp, ctypes.c_char_p, _sz], _i),
+    "d3d_device_alloc": ([_sz, _vpp], _i),
+    "d3d_device_free": ([_vp], _i),
+    "d3d_host_alloc": ([_sz, _vpp], _i),
+    "d3d_host_free": ([_vp], _i),
+    "d3d_memcpy": ([_vp, _vp, _sz, _vp], _i),
+    "d3d_stream_sync": ([_vp], _i),
+    "d3d_step": ([_vp, _vp, _vp, _vp, _vp], _i),
+    "d3d_run": ([_vp, _vpp, _vpp, _vp, _i, _vp], _i),
+    "d3d_run_host": ([_vp, _vp, _vp, _vp, _vp, _i, _vp,
+                      ctypes.POINTER(ctypes.c_float)], _i),
+    "d3d_analytic": ([_vp, _vp, ctypes.c_double, _vp], _i),
+    "d3d_compare": ([_vp, _vp, _i, _vp, _i, _sz, _dp, _vp], _i),
+    "d3d_check_device_errors": ([ctypes.POINTER(ctypes.c_uint)], _i),
+}
+
+_lib = None
+
+
+class D3DError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("d3d error %d: %s" % (code, msg))
+        self.code = code
+
+
+def declared_symbols(header: str = HEADER) -> list:
+    """Function names declared in include/d3d_b200.h."""
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(d3d_[a-z0-9_]+)\s*\(", text)))
+
+
+def build(force: bool = False) -> str:
+    from . import _build
+    return _build.build(force=force)
+
+
+def lib():
+    """The loaded library (built first if absent)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != D3D_OK:
+        raise D3DError(rc, lib().d3d_last_error().decode())
+
+
+def version() -> str:
+    return lib().d3d_version().decode()
+
+
+def launch_count() -> int:
+    return int(lib().d3d_launch_count())
+
+
+def np_dtype(dtype: int):
+    return np.float64 if dtype == F64 else np.float32
+
+
+def coefficients(nx, ny, nz, dtype=F32):
+    """Reference-constructor coefficients (ce,cw,cn,cs,ct,cb,cc) and geometry
+    (kappa,dx,dy,dz,kx,ky,kz,dt) in `dtype` -- a host-only entry point."""
+    c = np.zeros(7, np_dtype(dtype))
+    g = np.zeros(8, np_dtype(dtype))
+    check(lib().d3d_coefficients(nx, ny, nz, dtype, c.ctypes.data,
+                                 g.ctypes.data))
+    return c, g
+
+
+def _stream_handle(stream):
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def _torch_dtype(dtype):
+    import torch
+    return torch.float64 if dtype == F64 else torch.float32
+
+
+class Plan:
+    """A d3d_plan: one grid shape, precision and kernel choice."""
+
+    def __init__(self, nx, ny, nz, dtype=F32, kernel=KERNEL_AUTO, tb_depth=1,
+                 variant=None, zchunk=0):
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.dtype = dtype
+        self.kernel = kernel
+        self.tb_depth = tb_depth
+        h = ctypes.c_void_p()
+        check(lib().d3d_plan_create(nx, ny, nz, dtype, kernel, tb_depth,
+                                    ctypes.byref(h)))
+        self._h = h
+        if variant is not None or zchunk:
+            self.set_tile(variant or 0, zchunk)
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def n(self):
+        return self.nx * self.ny * self.nz
+
+    @property
+    def nbytes(self):
+        return self.n * (8 if self.dtype == F64 else 4)
+
+    def set_tile(self, variant, zchunk=0):
+        check(lib().d3d_plan_set_tile(self._h, variant, zchunk))
+
+    def info(self) -> dict:
+        import json
+        buf = ctypes.create_string_buffer(1024)
+        check(lib().d3d_plan_info(self._h, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().d3d_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- coefficient helpers -------------------------------------------
+    def reference_coefficients(self):
+        return coefficients(self.nx, self.ny, self.nz, self.dtype)[0]
+
+    def _coeff(self, coeff):
+        if coeff is None:
+            coeff = self.reference_coefficients()
+        c = np.ascontiguousarray(coeff, dtype=np_dtype(self.dtype))
+        assert c.shape == (7,)
+        return c
+
+    # --- compute entry points (device buffers: torch tensors) -----------
+    def empty(self):
+        import torch
+        return torch.empty((self.nz, self.ny, self.nx),
+                           dtype=_torch_dtype(self.dtype), device="cuda")
+
+    def _check_buf(self, t):
+        assert t.is_cuda and t.is_contiguous() and t.numel() == self.n
+        assert t.dtype == _torch_dtype(self.dtype)
+
+    def step(self, f1, f2, coeff=None, stream=None):
+        self._check_buf(f1)
+        self._check_buf(f2)
+        c = self._coeff(coeff)
+        check(lib().d3d_step(self._h, f1.data_ptr(), f2.data_ptr(),
+                             c.ctypes.data, _stream_handle(stream)))
+
+    def run(self, f1, f2, count, coeff=None, stream=None):
+        """`count` steps ping-ponging f1/f2; returns (result, other)."""
+        self._check_buf(f1)
+        self._check_buf(f2)
+        c = self._coeff(coeff)
+        a = ctypes.c_void_p(f1.data_ptr())
+        b = ctypes.c_void_p(f2.data_ptr())
+        check(lib().d3d_run(self._h, ctypes.byref(a), ctypes.byref(b),
+                            c.ctypes.data, count, _stream_handle(stream)))
+        if a.value == f1.data_ptr():
+            return f1, f2
+        return f2, f1
+
+    def run_host(self, host, f1, f2, count, coeff=None, stream=None):
+        """Diffusion3DCUDA::RunKernel semantics: host -> device, count steps,
+        result back into `host` (a C-contiguous numpy array, ideally
+        pinned).  Returns the kernel-only milliseconds."""
+        assert host.flags["C_CONTIGUOUS"] and host.size == self.n
+        assert host.dtype == np_dtype(self.dtype)
+        self._check_buf(f1)
+        self._check_buf(f2)
+        c = self._coeff(coeff)
+        ms = ctypes.c_float()
+        check(lib().d3d_run_host(self._h, host.ctypes.data, f1.data_ptr(),
+                                 f2.data_ptr(), c.ctypes.data, count,
+                                 _stream_handle(stream), ctypes.byref(ms)))
+        return ms.value
+
+    def analytic(self, out, time, stream=None):
+        self._check_buf(out)
+        check(lib().d3d_analytic(self._h, out.data_ptr(), float(time),
+                                 _stream_handle(stream)))
+
+    def compare(self, a, b, stream=None):
+        """FP64 (rms, max_abs, max_rel, sum(a)) of device field a vs b."""
+        import torch
+        assert a.numel() == b.numel()
+        dt = {torch.float32: F32, torch.float64: F64}
+        out = np.zeros(4, np.float64)
+        check(lib().d3d_compare(self._h, a.data_ptr(), dt[a.dtype],
+                                b.data_ptr(), dt[b.dtype], a.numel(),
+                                out.ctypes.data_as(_dp),
+                                _stream_handle(stream)))
+        return out
+
+
+def check_device_errors() -> int:
+    flags = ctypes.c_uint()
+    rc = lib().d3d_check_device_errors(ctypes.byref(flags))
+    if rc not in (D3D_OK, D3D_E_TIMEOUT):
+        check(rc)
+    return flags.value
+
+
+def pinned_empty(shape, dtype=np.float32):
+    """A numpy view of a pinned host buffer (torch pinned memory)."""
+    import torch
+    tdt = torch.float64 if np.dtype(dtype) == np.float64 else torch.float32
+    t = torch.empty(tuple(shape), dtype=tdt, pin_memory=True)
+    return t.numpy()

@@ -1,0 +1,455 @@
+// The C ABI of libd3d_b200.so (declared in include/d3d_b200.h).
+//
+// Host-side runtime around the kernels: plans (shape, dtype, kernel and
+// tile choice, cached TMA descriptors), the RunKernel-style step loops with
+// the reference's pointer swap, host<->device staging, error reporting.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "d3d_b200.h"
+#include "d3d_kernels.h"
+
+using d3d::kF32;
+using d3d::kF64;
+
+namespace {
+
+thread_local std::string g_last_error;
+std::atomic<unsigned long long> g_launches{0};
+
+// Kernels record bounded-wait failures here instead of trapping.
+__device__ unsigned g_dev_error_word;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  cudaGetLastError();  // clear a sticky-free error so the next call is clean
+  return fail(e == cudaErrorMemoryAllocation ? D3D_E_OOM : D3D_E_CUDA,
+              "%s: %s (%d)", what, cudaGetErrorString(e), (int)e);
+}
+
+#define D3D_TRY(call, what)                         \
+  do {                                              \
+    cudaError_t e__ = (call);                       \
+    if (e__ != cudaSuccess) return cuda_fail(e__, what); \
+  } while (0)
+
+unsigned* dev_error_ptr() {
+  static unsigned* ptrs[64] = {nullptr};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    return nullptr;
+  if (!ptrs[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_dev_error_word) != cudaSuccess)
+      return nullptr;
+    ptrs[dev] = static_cast<unsigned*>(p);
+  }
+  return ptrs[dev];
+}
+
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+bool valid_dims(int nx, int ny, int nz) {
+  if (nx < 1 || ny < 1 || nz < 1) return false;
+  // TMA coordinates and the generic kernel's grid are 32-bit; planes of up
+  // to 2^31 points and fields of up to 2^40 points are addressable.
+  if ((long long)nx * ny >= (1LL << 31)) return false;
+  if ((long long)nx * ny * nz >= (1LL << 40)) return false;
+  return true;
+}
+
+// Diffusion3D::Diffusion3D (diffusion3d.h:54-66): the same expressions,
+// evaluated with the same intermediate precisions as the reference when T
+// is float (double literals 0.1, 1.0, 2.0*pi promote, then narrow).
+template <typename T>
+void reference_coefficients(int nx, int ny, int nz, T* coeff, T* geom) {
+  const T kappa = (T)0.1;
+  const T l = (T)1.0;
+  const T dx = l / nx, dy = l / ny, dz = l / nz;
+  const T k = (T)(2.0 * 3.14159265358979323846);
+  const T dt = (T)(0.1 * dx * dx / kappa);
+  const T ce = kappa * dt / (dx * dx);
+  const T cn = kappa * dt / (dy * dy);
+  const T ct = kappa * dt / (dz * dz);
+  const T cc = (T)(1.0 - (ce + ce + cn + cn + ct + ct));
+  if (coeff) {
+    const T c[7] = {ce, ce, cn, cn, ct, ct, cc};
+    memcpy(coeff, c, sizeof c);
+  }
+  if (geom) {
+    const T g[8] = {kappa, dx, dy, dz, k, k, k, dt};
+    memcpy(geom, g, sizeof g);
+  }
+}
+
+}  // namespace
+
+struct d3d_plan_s {
+  int nx, ny, nz, dtype, kernel, tb_depth;
+  int variant;  // TMA tile variant
+  int zchunk;   // 0 = automatic
+  int device;
+  size_t n;
+  // Small cache of TMA descriptors keyed by (pointer, box rows).
+  struct MapEntry {
+    const void* ptr;
+    int box_x, box_y;
+    CUtensorMap map;
+  } maps[4];
+  int map_next;
+  double* cmp_scratch;  // device scratch for d3d_compare
+  cudaEvent_t ev[2];
+  d3d::LaunchInfo last;
+  const char* last_kernel;
+};
+
+namespace {
+
+int get_map(d3d_plan p, const void* ptr, int box_x, int box_y,
+            const CUtensorMap** out) {
+  for (auto& m : p->maps)
+    if (m.ptr == ptr && m.box_x == box_x && m.box_y == box_y) {
+      *out = &m.map;
+      return D3D_OK;
+    }
+  auto& m = p->maps[p->map_next];
+  p->map_next = (p->map_next + 1) % 4;
+  cudaError_t e = d3d::encode_field_map(&m.map, ptr, p->nx, p->ny, p->nz,
+                                        p->dtype, box_x, box_y);
+  if (e != cudaSuccess) {
+    m.ptr = nullptr;
+    return fail(D3D_E_CUDA, "cuTensorMapEncodeTiled failed for %p", ptr);
+  }
+  m.ptr = ptr;
+  m.box_x = box_x;
+  m.box_y = box_y;
+  *out = &m.map;
+  return D3D_OK;
+}
+
+int check_device(d3d_plan p) {
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (dev != p->device)
+    return fail(D3D_E_INVALID, "plan bound to device %d, current is %d",
+                p->device, dev);
+  return D3D_OK;
+}
+
+// One single-step launch, choosing the TMA path when the buffer allows it.
+int step_once(d3d_plan p, const void* f1, void* f2, const void* coeff,
+              cudaStream_t s) {
+  const bool use_tma = p->kernel != D3D_KERNEL_GENERIC &&
+                       d3d::tma_eligible(f1, p->nx, p->ny, p->dtype);
+  if (p->kernel == D3D_KERNEL_TMA && !use_tma)
+    return fail(D3D_E_UNSUPPORTED,
+                "TMA kernel needs a 16-byte aligned buffer and nx*%d %% 16 == 0",
+                (int)d3d::dtype_size(p->dtype));
+  if (use_tma) {
+    const CUtensorMap* map = nullptr;
+    int rc = get_map(p, f1, d3d::tma_box_x(p->dtype),
+                     d3d::tma_box_y(p->variant), &map);
+    if (rc) return rc;
+    D3D_TRY(d3d::launch_step_tma(*map, f2, p->nx, p->ny, p->nz, coeff,
+                                 p->dtype, p->variant, p->zchunk, s,
+                                 dev_error_ptr(), &p->last),
+            "step_tma launch");
+    p->last_kernel = "step_tma";
+  } else {
+    D3D_TRY(d3d::launch_step_generic(f1, f2, p->nx, p->ny, p->nz, coeff,
+                                     p->dtype, s, &p->last),
+            "step_generic launch");
+    p->last_kernel = "step_generic";
+  }
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return D3D_OK;
+}
+
+int tb_pass(d3d_plan p, const void* f1, void* f2, const void* coeff,
+            cudaStream_t s) {
+  const CUtensorMap* map = nullptr;
+  int rc = get_map(p, f1, d3d::tb_box_x(p->dtype, p->tb_depth),
+                   d3d::tb_box_y(p->tb_depth),
+                   &map);
+  if (rc) return rc;
+  D3D_TRY(d3d::launch_steps_tb(*map, f2, p->nx, p->ny, p->nz, coeff, p->dtype,
+                               p->tb_depth, p->zchunk, s, dev_error_ptr(),
+                               &p->last),
+          "temporal-blocking launch");
+  p->last_kernel = "steps_tb";
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return D3D_OK;
+}
+
+int run_loop(d3d_plan p, void** f1, void** f2, const void* coeff, int count,
+             cudaStream_t s) {
+  int done = 0;
+  if (p->kernel == D3D_KERNEL_TB && p->tb_depth > 1 &&
+      d3d::tma_eligible(*f1, p->nx, p->ny, p->dtype) &&
+      d3d::tma_eligible(*f2, p->nx, p->ny, p->dtype)) {
+    for (; done + p->tb_depth <= count; done += p->tb_depth) {
+      int rc = tb_pass(p, *f1, *f2, coeff, s);
+      if (rc) return rc;
+      std::swap(*f1, *f2);
+    }
+  }
+  for (; done < count; ++done) {
+    int rc = step_once(p, *f1, *f2, coeff, s);
+    if (rc) return rc;
+    std::swap(*f1, *f2);
+  }
+  return D3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* d3d_version(void) { return "d3d_b200 1.0 (sm_100a)"; }
+
+const char* d3d_last_error(void) { return g_last_error.c_str(); }
+
+unsigned long long d3d_launch_count(void) { return g_launches.load(); }
+
+int d3d_coefficients(int nx, int ny, int nz, int dtype, void* coeff7,
+                     void* geom8) {
+  if (!valid_dims(nx, ny, nz))
+    return fail(D3D_E_INVALID, "bad dims %dx%dx%d", nx, ny, nz);
+  if (dtype == kF64)
+    reference_coefficients<double>(nx, ny, nz, static_cast<double*>(coeff7),
+                                   static_cast<double*>(geom8));
+  else if (dtype == kF32)
+    reference_coefficients<float>(nx, ny, nz, static_cast<float*>(coeff7),
+                                  static_cast<float*>(geom8));
+  else
+    return fail(D3D_E_INVALID, "bad dtype %d", dtype);
+  return D3D_OK;
+}
+
+int d3d_plan_create(int nx, int ny, int nz, int dtype, int kernel,
+                    int tb_depth, d3d_plan* out) {
+  if (!out) return fail(D3D_E_INVALID, "out is NULL");
+  *out = nullptr;
+  if (!valid_dims(nx, ny, nz))
+    return fail(D3D_E_INVALID, "bad dims %dx%dx%d", nx, ny, nz);
+  if (dtype != kF32 && dtype != kF64)
+    return fail(D3D_E_INVALID, "bad dtype %d", dtype);
+  if (kernel < D3D_KERNEL_AUTO || kernel > D3D_KERNEL_TB)
+    return fail(D3D_E_INVALID, "bad kernel %d", kernel);
+  if (kernel == D3D_KERNEL_TB && !d3d::tb_supported(tb_depth, dtype))
+    return fail(D3D_E_UNSUPPORTED, "temporal blocking depth %d unsupported",
+                tb_depth);
+  int dev = 0;
+  D3D_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+  d3d_plan p = new (std::nothrow) d3d_plan_s();
+  if (!p) return fail(D3D_E_OOM, "plan allocation");
+  p->nx = nx;
+  p->ny = ny;
+  p->nz = nz;
+  p->dtype = dtype;
+  p->kernel = kernel;
+  p->tb_depth = kernel == D3D_KERNEL_TB ? tb_depth : 1;
+  p->variant = 0;
+  p->zchunk = 0;
+  p->device = dev;
+  p->n = (size_t)nx * ny * nz;
+  p->last_kernel = "";
+  for (auto& m : p->maps) m.ptr = nullptr;
+  cudaError_t e = cudaEventCreate(&p->ev[0]);
+  if (e == cudaSuccess) e = cudaEventCreate(&p->ev[1]);
+  if (e != cudaSuccess) {
+    delete p;
+    return cuda_fail(e, "cudaEventCreate");
+  }
+  *out = p;
+  return D3D_OK;
+}
+
+int d3d_plan_set_tile(d3d_plan p, int variant, int zchunk) {
+  if (!p) return fail(D3D_E_INVALID, "plan is NULL");
+  if (variant < 0 || variant >= d3d::kNumTmaVariants || zchunk < 0)
+    return fail(D3D_E_INVALID, "bad tile variant %d / zchunk %d", variant,
+                zchunk);
+  p->variant = variant;
+  p->zchunk = zchunk;
+  for (auto& m : p->maps) m.ptr = nullptr;  // box height may change
+  return D3D_OK;
+}
+
+int d3d_plan_destroy(d3d_plan p) {
+  if (!p) return D3D_OK;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != p->device) cudaSetDevice(p->device);
+  if (p->cmp_scratch) cudaFree(p->cmp_scratch);
+  cudaEventDestroy(p->ev[0]);
+  cudaEventDestroy(p->ev[1]);
+  if (prev >= 0 && prev != p->device) cudaSetDevice(prev);
+  delete p;
+  return D3D_OK;
+}
+
+int d3d_plan_info(d3d_plan p, char* buf, size_t len) {
+  if (!p || !buf) return fail(D3D_E_INVALID, "NULL argument");
+  const auto& L = p->last;
+  snprintf(buf, len,
+           "{\"nx\": %d, \"ny\": %d, \"nz\": %d, \"dtype\": \"%s\", "
+           "\"kernel\": %d, \"tb_depth\": %d, \"variant\": %d, "
+           "\"zchunk\": %d, \"device\": %d, \"last_kernel\": \"%s\", "
+           "\"grid\": [%d, %d, %d], \"block\": %d, \"smem\": %d, "
+           "\"launch_zchunk\": %d, \"ctas_per_sm\": %d}",
+           p->nx, p->ny, p->nz, p->dtype == kF64 ? "f64" : "f32", p->kernel,
+           p->tb_depth, p->variant, p->zchunk, p->device, p->last_kernel,
+           L.grid_x, L.grid_y, L.grid_z, L.block, L.smem_bytes, L.zchunk,
+           L.ctas_per_sm);
+  return D3D_OK;
+}
+
+int d3d_device_alloc(size_t bytes, void** ptr) {
+  if (!ptr) return fail(D3D_E_INVALID, "ptr is NULL");
+  D3D_TRY(cudaMalloc(ptr, bytes), "cudaMalloc");
+  return D3D_OK;
+}
+
+int d3d_device_free(void* ptr) {
+  D3D_TRY(cudaFree(ptr), "cudaFree");
+  return D3D_OK;
+}
+
+int d3d_host_alloc(size_t bytes, void** ptr) {
+  if (!ptr) return fail(D3D_E_INVALID, "ptr is NULL");
+  D3D_TRY(cudaMallocHost(ptr, bytes), "cudaMallocHost");
+  return D3D_OK;
+}
+
+int d3d_host_free(void* ptr) {
+  D3D_TRY(cudaFreeHost(ptr), "cudaFreeHost");
+  return D3D_OK;
+}
+
+int d3d_memcpy(void* dst, const void* src, size_t bytes, void* stream) {
+  D3D_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault,
+                          as_stream(stream)),
+          "cudaMemcpyAsync");
+  return D3D_OK;
+}
+
+int d3d_stream_sync(void* stream) {
+  D3D_TRY(cudaStreamSynchronize(as_stream(stream)), "cudaStreamSynchronize");
+  return D3D_OK;
+}
+
+int d3d_step(d3d_plan p, const void* f1, void* f2, const void* coeff,
+             void* stream) {
+  if (!p || !f1 || !f2 || !coeff) return fail(D3D_E_INVALID, "NULL argument");
+  if (f1 == f2) return fail(D3D_E_INVALID, "f1 and f2 alias");
+  int rc = check_device(p);
+  if (rc) return rc;
+  return step_once(p, f1, f2, coeff, as_stream(stream));
+}
+
+int d3d_run(d3d_plan p, void** f1, void** f2, const void* coeff, int count,
+            void* stream) {
+  if (!p || !f1 || !f2 || !*f1 || !*f2 || !coeff)
+    return fail(D3D_E_INVALID, "NULL argument");
+  if (*f1 == *f2) return fail(D3D_E_INVALID, "f1 and f2 alias");
+  if (count < 0) return fail(D3D_E_INVALID, "negative count %d", count);
+  int rc = check_device(p);
+  if (rc) return rc;
+  return run_loop(p, f1, f2, coeff, count, as_stream(stream));
+}
+
+int d3d_run_host(d3d_plan p, void* host_f1, void* dev_f1, void* dev_f2,
+                 const void* coeff, int count, void* stream,
+                 float* kernel_ms) {
+  if (!p || !host_f1 || !dev_f1 || !dev_f2 || !coeff)
+    return fail(D3D_E_INVALID, "NULL argument");
+  if (dev_f1 == dev_f2) return fail(D3D_E_INVALID, "f1 and f2 alias");
+  if (count < 0) return fail(D3D_E_INVALID, "negative count %d", count);
+  int rc = check_device(p);
+  if (rc) return rc;
+  cudaStream_t s = as_stream(stream);
+  const size_t bytes = p->n * d3d::dtype_size(p->dtype);
+  D3D_TRY(cudaMemcpyAsync(dev_f1, host_f1, bytes, cudaMemcpyHostToDevice, s),
+          "H2D copy");
+  D3D_TRY(cudaEventRecord(p->ev[0], s), "cudaEventRecord");
+  void* a = dev_f1;
+  void* b = dev_f2;
+  rc = run_loop(p, &a, &b, coeff, count, s);
+  if (rc) return rc;
+  D3D_TRY(cudaEventRecord(p->ev[1], s), "cudaEventRecord");
+  D3D_TRY(cudaMemcpyAsync(host_f1, a, bytes, cudaMemcpyDeviceToHost, s),
+          "D2H copy");
+  D3D_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  if (kernel_ms)
+    D3D_TRY(cudaEventElapsedTime(kernel_ms, p->ev[0], p->ev[1]),
+            "cudaEventElapsedTime");
+  return D3D_OK;
+}
+
+int d3d_analytic(d3d_plan p, void* out, double time, void* stream) {
+  if (!p || !out) return fail(D3D_E_INVALID, "NULL argument");
+  int rc = check_device(p);
+  if (rc) return rc;
+  double g[8];
+  reference_coefficients<double>(p->nx, p->ny, p->nz, nullptr, g);
+  D3D_TRY(d3d::launch_analytic(out, p->dtype, p->nx, p->ny, p->nz, g[4], g[5],
+                               g[6], g[1], g[2], g[3], g[0], time,
+                               as_stream(stream)),
+          "analytic launch");
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return D3D_OK;
+}
+
+int d3d_compare(d3d_plan p, const void* a, int a_dtype, const void* b,
+                int b_dtype, size_t n, double out[4], void* stream) {
+  if (!p || !a || !b || !out) return fail(D3D_E_INVALID, "NULL argument");
+  if ((a_dtype != kF32 && a_dtype != kF64) ||
+      (b_dtype != kF32 && b_dtype != kF64))
+    return fail(D3D_E_INVALID, "bad dtype");
+  int rc = check_device(p);
+  if (rc) return rc;
+  cudaStream_t s = as_stream(stream);
+  if (!p->cmp_scratch)
+    D3D_TRY(cudaMalloc(&p->cmp_scratch, d3d::compare_scratch_bytes()),
+            "cudaMalloc (compare scratch)");
+  D3D_TRY(d3d::launch_compare(a, a_dtype, b, b_dtype, n, p->cmp_scratch, s),
+          "compare launch");
+  g_launches.fetch_add(2, std::memory_order_relaxed);
+  D3D_TRY(cudaMemcpyAsync(out, p->cmp_scratch, 4 * sizeof(double),
+                          cudaMemcpyDeviceToHost, s),
+          "D2H copy");
+  D3D_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  return D3D_OK;
+}
+
+int d3d_check_device_errors(unsigned* flags_out) {
+  D3D_TRY(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+  unsigned* p = dev_error_ptr();
+  if (!p) return fail(D3D_E_CUDA, "cannot resolve device error word");
+  unsigned v = 0;
+  D3D_TRY(cudaMemcpy(&v, p, sizeof v, cudaMemcpyDeviceToHost), "D2H copy");
+  if (v) D3D_TRY(cudaMemset(p, 0, sizeof v), "cudaMemset");
+  if (flags_out) *flags_out = v;
+  if (v) return fail(D3D_E_TIMEOUT, "device error flags 0x%x", v);
+  return D3D_OK;
+}
+
+}  // extern "C"

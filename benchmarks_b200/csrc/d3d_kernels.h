@@ -1,0 +1,76 @@
+// Host-side declarations of the kernel launchers inside libd3d_b200.so.
+// Not part of the public C ABI (include/d3d_b200.h is).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+namespace d3d {
+
+enum Dtype { kF32 = 0, kF64 = 1 };
+
+inline size_t dtype_size(int dtype) { return dtype == kF64 ? 8 : 4; }
+
+// Tile configurations of the TMA-staged single-step kernel.
+struct TmaVariant {
+  int by;      // rows of the xy tile
+  int stages;  // planes in the shared-memory ring
+};
+constexpr int kNumTmaVariants = 5;
+const TmaVariant& tma_variant(int i);
+
+// Launch geometry actually used (for reporting and for the autotuner).
+struct LaunchInfo {
+  int grid_x, grid_y, grid_z;
+  int block;
+  int smem_bytes;
+  int zchunk;
+  int ctas_per_sm;
+};
+
+bool tma_eligible(const void* ptr, int nx, int ny, int dtype);
+
+// Encodes a 3-D tiled tensor map over a field for the TMA kernels.
+// box = (tile_x + 2*halo_x) x (tile_y + 2*halo_y) x 1.
+cudaError_t encode_field_map(CUtensorMap* map, const void* ptr, int nx, int ny,
+                             int nz, int dtype, int box_x, int box_y);
+
+// One time step, f2 = stencil(f1), with the TMA-staged z-march.
+cudaError_t launch_step_tma(const CUtensorMap& src, void* f2, int nx, int ny,
+                            int nz, const void* coef, int dtype, int variant,
+                            int zchunk_override, cudaStream_t stream,
+                            unsigned* dev_err, LaunchInfo* info);
+int tma_box_x(int dtype);
+int tma_box_y(int variant);
+
+// One time step with the generic kernel (any shape, any alignment).
+cudaError_t launch_step_generic(const void* f1, void* f2, int nx, int ny,
+                                int nz, const void* coef, int dtype,
+                                cudaStream_t stream, LaunchInfo* info);
+
+// k fused time steps (temporal blocking), f2 = stencil^k(f1).
+cudaError_t launch_steps_tb(const CUtensorMap& src, void* f2, int nx, int ny,
+                            int nz, const void* coef, int dtype, int k,
+                            int zchunk_override, cudaStream_t stream,
+                            unsigned* dev_err, LaunchInfo* info);
+int tb_box_x(int dtype, int k);
+int tb_box_y(int k);
+bool tb_supported(int k, int dtype);
+
+// FP64-accumulated comparison of two device fields (any dtype pair):
+// out[0] = rms(a-b), out[1] = max|a-b|, out[2] = max|a-b|/|b|, out[3] = sum(a).
+// `scratch` holds `compare_scratch_bytes()` bytes of device memory.
+size_t compare_scratch_bytes();
+cudaError_t launch_compare(const void* a, int a_dtype, const void* b,
+                           int b_dtype, size_t n, double* scratch,
+                           cudaStream_t stream);
+
+// Analytic solution (the reference's Initialize, computed in FP64 on the
+// device) written in `dtype` at `time`.
+cudaError_t launch_analytic(void* out, int dtype, int nx, int ny, int nz,
+                            double kx, double ky, double kz, double dx,
+                            double dy, double dz, double kappa, double time,
+                            cudaStream_t stream);
+
+}  // namespace d3d

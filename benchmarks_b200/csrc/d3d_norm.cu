@@ -1,0 +1,175 @@
+// Device-side error norms and the analytic field.
+//
+// The reference reports accuracy on the host: GetCorrectAnswer rebuilds the
+// analytic field with Initialize(t = count*dt) (diffusion3d.h:113-120) and
+// Baseline::GetAccuracy sums the squared error in float (baseline.cc:51-60).
+// These kernels provide the FP64 error report beside it, on the device:
+//   * analytic_kernel -- the same closed form, evaluated in double;
+//   * compare kernels  -- rms, max-abs, max-rel and a checksum accumulated
+//     in double over two device fields of any dtype pair, in a fixed
+//     reduction order (deterministic for a given device).
+#include <cfloat>
+
+#include "d3d_common.cuh"
+#include "d3d_kernels.h"
+
+namespace d3d {
+
+namespace {
+
+constexpr int kCmpThreads = 256;
+constexpr int kCmpBlocks = 1024;  // partials in scratch: 4 doubles each
+
+template <typename T>
+__device__ __forceinline__ double ld_as_double(const void* p, size_t i) {
+  return (double)static_cast<const T*>(p)[i];
+}
+
+struct Acc {
+  double ss, mx, mr, sa;
+};
+
+__device__ __forceinline__ void acc_merge(Acc& a, const Acc& b) {
+  a.ss += b.ss;
+  a.mx = fmax(a.mx, b.mx);
+  a.mr = fmax(a.mr, b.mr);
+  a.sa += b.sa;
+}
+
+__device__ Acc block_reduce(Acc v) {
+  __shared__ Acc sh[kCmpThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    Acc u;
+    u.ss = __shfl_down_sync(0xffffffffu, v.ss, o);
+    u.mx = __shfl_down_sync(0xffffffffu, v.mx, o);
+    u.mr = __shfl_down_sync(0xffffffffu, v.mr, o);
+    u.sa = __shfl_down_sync(0xffffffffu, v.sa, o);
+    acc_merge(v, u);
+  }
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  Acc r = {0, 0, 0, 0};
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < kCmpThreads / 32; ++w) acc_merge(r, sh[w]);
+  }
+  return r;
+}
+
+template <typename TA, typename TB>
+__global__ void __launch_bounds__(kCmpThreads)
+    compare_partial_kernel(const void* a, const void* b, size_t n,
+                           double* partial) {
+  Acc v = {0, 0, 0, 0};
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += stride) {
+    const double x = ld_as_double<TA>(a, i);
+    const double y = ld_as_double<TB>(b, i);
+    const double d = x - y;
+    const double ad = fabs(d);
+    const double den = fmax(fabs(y), 1e-300);
+    v.ss += d * d;
+    v.mx = fmax(v.mx, ad);
+    v.mr = fmax(v.mr, ad / den);
+    v.sa += x;
+  }
+  Acc r = block_reduce(v);
+  if (threadIdx.x == 0) {
+    double* p = partial + 4 * (size_t)blockIdx.x;
+    p[0] = r.ss;
+    p[1] = r.mx;
+    p[2] = r.mr;
+    p[3] = r.sa;
+  }
+}
+
+__global__ void __launch_bounds__(kCmpThreads)
+    compare_final_kernel(const double* partial, int nparts, size_t n,
+                         double* out) {
+  Acc v = {0, 0, 0, 0};
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+    const double* p = partial + 4 * (size_t)i;
+    Acc u = {p[0], p[1], p[2], p[3]};
+    acc_merge(v, u);
+  }
+  Acc r = block_reduce(v);
+  if (threadIdx.x == 0) {
+    out[0] = n ? sqrt(r.ss / (double)n) : 0.0;
+    out[1] = r.mx;
+    out[2] = r.mr;
+    out[3] = r.sa;
+  }
+}
+
+template <typename T>
+__global__ void analytic_kernel(T* out, int nx, int ny, int nz, double kx,
+                                double ky, double kz, double dx, double dy,
+                                double dz, double ax, double ay, double az) {
+  const size_t n = (size_t)nx * ny * nz;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += stride) {
+    const int jx = (int)(i % nx);
+    const int jy = (int)((i / nx) % ny);
+    const int jz = (int)(i / ((size_t)nx * ny));
+    const double x = dx * (jx + 0.5), y = dy * (jy + 0.5), z = dz * (jz + 0.5);
+    out[i] = (T)(0.125 * (1.0 - ax * cos(kx * x)) * (1.0 - ay * cos(ky * y)) *
+                 (1.0 - az * cos(kz * z)));
+  }
+}
+
+template <typename TA>
+cudaError_t launch_partial(const void* a, const void* b, int b_dtype, size_t n,
+                           double* partial, int blocks, cudaStream_t s) {
+  if (b_dtype == kF64)
+    compare_partial_kernel<TA, double>
+        <<<blocks, kCmpThreads, 0, s>>>(a, b, n, partial);
+  else
+    compare_partial_kernel<TA, float>
+        <<<blocks, kCmpThreads, 0, s>>>(a, b, n, partial);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t compare_scratch_bytes() { return (size_t)(kCmpBlocks + 1) * 4 * 8; }
+
+// Result lands in scratch[0..3] (the partials live after it).
+cudaError_t launch_compare(const void* a, int a_dtype, const void* b,
+                           int b_dtype, size_t n, double* scratch,
+                           cudaStream_t stream) {
+  const int blocks = kCmpBlocks;
+  double* partial = scratch + 4;
+  cudaError_t e = a_dtype == kF64
+                      ? launch_partial<double>(a, b, b_dtype, n, partial,
+                                               blocks, stream)
+                      : launch_partial<float>(a, b, b_dtype, n, partial,
+                                              blocks, stream);
+  if (e != cudaSuccess) return e;
+  compare_final_kernel<<<1, kCmpThreads, 0, stream>>>(partial, blocks, n,
+                                                      scratch);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_analytic(void* out, int dtype, int nx, int ny, int nz,
+                            double kx, double ky, double kz, double dx,
+                            double dy, double dz, double kappa, double time,
+                            cudaStream_t stream) {
+  const double ax = exp(-kappa * time * (kx * kx));
+  const double ay = exp(-kappa * time * (ky * ky));
+  const double az = exp(-kappa * time * (kz * kz));
+  const int threads = 256, blocks = 148 * 8;
+  if (dtype == kF64)
+    analytic_kernel<double><<<blocks, threads, 0, stream>>>(
+        static_cast<double*>(out), nx, ny, nz, kx, ky, kz, dx, dy, dz, ax, ay,
+        az);
+  else
+    analytic_kernel<float><<<blocks, threads, 0, stream>>>(
+        static_cast<float*>(out), nx, ny, nz, kx, ky, kz, dx, dy, dz, ax, ay,
+        az);
+  return cudaGetLastError();
+}
+
+}  // namespace d3d

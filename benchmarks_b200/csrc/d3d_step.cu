@@ -1,0 +1,413 @@
+// Single-step diffusion3d kernels for sm_100a.
+//
+// Replaces the reference's per-step kernels (diffusion3d_cuda.cu:13-45 and
+// its optimised siblings, e.g. the b/c/t register queue of :129-170 and the
+// halo'd shared tiles of diffusion3d_cuda_shared1.cu:10-80) with:
+//
+//  * step_tma_kernel  -- the HBM-roofline path.  Each CTA owns a BX x BY xy
+//    tile and marches a z-chunk.  One thread issues a TMA 3-D box load per
+//    z-plane (tile + 1-row y halo + a 16-byte x halo) into a ring of
+//    shared-memory stages completed through mbarriers; the other planes of
+//    the ring are in flight while the CTA computes.  b and c planes of each
+//    thread's 16-byte column segment live in registers (the reference's
+//    t1/t2/t3 queue), x neighbours come from warp shuffles, y neighbours
+//    and the next plane from shared memory, and every output row segment
+//    is a 128-bit coalesced store.
+//
+//  * step_generic_kernel -- any shape and alignment (TMA needs 16-byte row
+//    pitches): 32x8 tiles, halo cells fetched with clamped coordinates so
+//    the replicated boundary falls out of the addressing.
+//
+// Both evaluate d3d::point (exact reference order, no FMA), so results are
+// bit-identical to Diffusion3DOpenMP::RunKernel.
+#include <algorithm>
+#include <cstdio>
+
+#include "d3d_common.cuh"
+#include "d3d_kernels.h"
+
+namespace d3d {
+
+// ---------------------------------------------------------------------------
+// TMA-staged z-march
+// ---------------------------------------------------------------------------
+template <typename T, int BY, int S>
+struct StepTmaCfg {
+  static constexpr int WARPS = 8;
+  static constexpr int THREADS = WARPS * 32;
+  static constexpr int V = 16 / sizeof(T);  // elements per 16-byte segment
+  static constexpr int BX = 32 * V;         // one warp spans the tile width
+  static constexpr int HX = V;              // 16-byte x halo on each side
+  static constexpr int P = BX + 2 * HX;     // smem row pitch (elements)
+  static constexpr int R = BY + 2;          // rows per stage (1-row y halo)
+  static constexpr int RPW = BY / WARPS;    // tile rows per warp
+  static constexpr int STAGE_BYTES_RAW = P * R * (int)sizeof(T);
+  static constexpr int STAGE_BYTES = (STAGE_BYTES_RAW + 127) / 128 * 128;
+  static constexpr int STAGE_ELEMS = STAGE_BYTES / (int)sizeof(T);
+  static constexpr int SMEM = S * STAGE_BYTES + S * 8 + 128;
+  static_assert(BY % WARPS == 0, "BY must be a multiple of the warp count");
+  static_assert(P <= 256 && R <= 256, "TMA box dimensions are at most 256");
+  static_assert(S >= 4, "the ring keeps planes z, z+1, z+2 and one in flight");
+};
+
+template <typename T, int BY, int S>
+__global__ void __launch_bounds__(StepTmaCfg<T, BY, S>::THREADS)
+    step_tma_kernel(const __grid_constant__ CUtensorMap src,
+                    T* __restrict__ dst, int nx, int ny, int nz, Coef<T> k,
+                    int zchunk, unsigned* __restrict__ dev_err) {
+  using C = StepTmaCfg<T, BY, S>;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  T* stages = reinterpret_cast<T*>(base);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + S * C::STAGE_BYTES);
+
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int x0 = blockIdx.x * C::BX;
+  const int y0 = blockIdx.y * BY;
+  const int z0 = blockIdx.z * zchunk;
+  const int z1 = min(nz, z0 + zchunk);
+  if (z0 >= z1) return;
+  const int pbase = z0 > 0 ? z0 - 1 : 0;  // first plane loaded (b of z0)
+  const int plast = min(z1, nz - 1);      // last plane needed (t of z1-1)
+
+  auto stage_of = [&](int p) { return (p - pbase) % S; };
+  auto parity_of = [&](int p) { return (unsigned)(((p - pbase) / S) & 1); };
+  auto issue = [&](int p) {
+    const int s = stage_of(p);
+    mbar_arrive_expect_tx(&bars[s], C::STAGE_BYTES_RAW);
+    tma_load_3d(stages + s * C::STAGE_ELEMS, &src, &bars[s], x0 - C::HX,
+                y0 - 1, p);
+  };
+
+  if (threadIdx.x == 0) {
+    tma_prefetch_desc(&src);
+    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int p = pbase; p <= plast && p < pbase + S; ++p) issue(p);
+  }
+
+  const int xg = x0 + C::V * lane;   // first x of this thread's segment
+  const int col = C::HX + C::V * lane;  // its smem column
+  const bool x_lo = (xg == 0);
+  const bool x_hi = (xg + C::V - 1 == nx - 1);
+
+  V16<T> creg[C::RPW], breg[C::RPW];
+  // Planes issued but not yet waited for, drained if a wait runs out.
+  int drain_lo = pbase, drain_hi = min(plast, pbase + S - 1);
+
+  // Prologue: planes z0 (c) and z0-1 (b), and z0+1 (t of the first step).
+  bool ok = mbar_wait_bounded(&bars[stage_of(z0)], parity_of(z0));
+  if (z0 > 0) ok = ok && mbar_wait_bounded(&bars[stage_of(z0 - 1)],
+                                           parity_of(z0 - 1));
+  if (z0 + 1 <= plast)
+    ok = ok && mbar_wait_bounded(&bars[stage_of(z0 + 1)], parity_of(z0 + 1));
+  if (!__syncthreads_and(ok)) {
+    if (threadIdx.x == 0) atomicOr(dev_err, kDevWaitTimeout);
+    goto drain;
+  }
+  {
+    const T* sc = stages + stage_of(z0) * C::STAGE_ELEMS;
+    const T* sb = stages + stage_of(pbase) * C::STAGE_ELEMS;
+#pragma unroll
+    for (int r = 0; r < C::RPW; ++r) {
+      const int row = warp * C::RPW + r;
+      creg[r] = ld16_shared(sc + (row + 1) * C::P + col);
+      breg[r] = (z0 > 0) ? ld16_shared(sb + (row + 1) * C::P + col) : creg[r];
+    }
+  }
+  __syncthreads();
+  if (z0 > 0 && threadIdx.x == 0 && pbase + S <= plast) issue(pbase + S);
+
+  for (int z = z0; z < z1; ++z) {
+    const bool has_t = (z + 1 < nz);
+    const T* sc = stages + stage_of(z) * C::STAGE_ELEMS;
+    const T* st = stages + stage_of(has_t ? z + 1 : z) * C::STAGE_ELEMS;
+    T* out_plane = dst + (size_t)z * ny * nx;
+#pragma unroll
+    for (int r = 0; r < C::RPW; ++r) {
+      const int row = warp * C::RPW + r;
+      const int yg = y0 + row;
+      const V16<T> c = creg[r];
+      const V16<T> t = has_t ? ld16_shared(st + (row + 1) * C::P + col) : c;
+      const V16<T> n = (yg == 0) ? c : ld16_shared(sc + row * C::P + col);
+      const V16<T> s =
+          (yg == ny - 1) ? c : ld16_shared(sc + (row + 2) * C::P + col);
+      T wl = __shfl_up_sync(0xffffffffu, c.e[C::V - 1], 1);
+      T er = __shfl_down_sync(0xffffffffu, c.e[0], 1);
+      if (lane == 0) wl = sc[(row + 1) * C::P + col - 1];
+      if (lane == 31) er = sc[(row + 1) * C::P + col + C::V];
+      if (x_lo) wl = c.e[0];
+      if (x_hi) er = c.e[C::V - 1];
+      V16<T> o;
+#pragma unroll
+      for (int i = 0; i < C::V; ++i) {
+        const T w = (i == 0) ? wl : c.e[i - 1];
+        const T e = (i == C::V - 1) ? er : c.e[i + 1];
+        o.e[i] = point(k, c.e[i], w, e, s.e[i], n.e[i], breg[r].e[i], t.e[i]);
+      }
+      if (yg < ny && xg < nx) st16_global(out_plane + (size_t)yg * nx + xg, o);
+      breg[r] = c;
+      creg[r] = t;
+    }
+    // Plane z+2 is the t plane of the next step; wait for it before the
+    // barrier that releases plane z's stage to the producer.
+    bool ok2 = true;
+    if (z + 2 <= plast && z + 1 < z1)
+      ok2 = mbar_wait_bounded(&bars[stage_of(z + 2)], parity_of(z + 2));
+    if (!__syncthreads_and(ok2)) {
+      if (threadIdx.x == 0) atomicOr(dev_err, kDevWaitTimeout);
+      drain_lo = z + 2;
+      drain_hi = min(plast, z + S - 1);
+      goto drain;
+    }
+    if (threadIdx.x == 0 && z + S <= plast) issue(z + S);
+  }
+  return;
+
+drain:
+  // A wait ran out: let every load this CTA issued and has not yet waited
+  // for land before its shared memory is released.  Bounded as well.
+  if (threadIdx.x == 0) {
+    for (int p = drain_lo; p <= drain_hi; ++p) {
+      bool done = false;
+      for (unsigned i = 0; i < (kMaxWaitIters >> 4) && !done; ++i)
+        done = mbar_try_wait(&bars[stage_of(p)], parity_of(p));
+      if (!done) {
+        atomicOr(dev_err, kDevDrainTimeout);
+        break;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Generic kernel: any nx, ny, nz, any alignment.
+// ---------------------------------------------------------------------------
+constexpr int kGenBX = 32;
+constexpr int kGenBY = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(kGenBX* kGenBY)
+    step_generic_kernel(const T* __restrict__ src, T* __restrict__ dst,
+                        int nx, int ny, int nz, Coef<T> k, int zchunk) {
+  __shared__ T tile[kGenBY + 2][kGenBX + 2];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int xg = blockIdx.x * kGenBX + tx;
+  const int yg = blockIdx.y * kGenBY + ty;
+  const int z0 = blockIdx.z * zchunk;
+  const int z1 = min(nz, z0 + zchunk);
+  if (z0 >= z1) return;
+  // Clamped coordinates: out-of-domain halo cells read the edge cell, which
+  // is exactly the reference's replicated-neighbour rule.
+  const int xc = min(xg, nx - 1);
+  const int yc = min(yg, ny - 1);
+  const size_t xy = (size_t)nx * ny;
+  const T* col = src + (size_t)yc * nx + xc;
+  const bool edge_w = (tx == 0), edge_e = (tx == kGenBX - 1);
+  const bool edge_n = (ty == 0), edge_s = (ty == kGenBY - 1);
+  const int xw = max(xg - 1, 0), xe = min(xg + 1, nx - 1);
+  const int yn = max(yg - 1, 0), ys = min(yg + 1, ny - 1);
+  const int xwc = min(xw, nx - 1), xec = min(xe, nx - 1);
+  const int ync = min(yn, ny - 1), ysc = min(ys, ny - 1);
+
+  T b = __ldg(col + (size_t)max(z0 - 1, 0) * xy);
+  T c = __ldg(col + (size_t)z0 * xy);
+  for (int z = z0; z < z1; ++z) {
+    const T t = __ldg(col + (size_t)min(z + 1, nz - 1) * xy);
+    const T* plane = src + (size_t)z * xy;
+    tile[ty + 1][tx + 1] = c;
+    if (edge_w) tile[ty + 1][0] = __ldg(plane + (size_t)yc * nx + xwc);
+    if (edge_e) tile[ty + 1][kGenBX + 1] = __ldg(plane + (size_t)yc * nx + xec);
+    if (edge_n) tile[0][tx + 1] = __ldg(plane + (size_t)ync * nx + xc);
+    if (edge_s) tile[kGenBY + 1][tx + 1] = __ldg(plane + (size_t)ysc * nx + xc);
+    __syncthreads();
+    // Inside the tile the neighbour cell is the tile cell; at a domain
+    // edge the clamped load above already holds the centre value.  A tile
+    // cell beyond the domain (xg >= nx) holds a clamped copy, and only
+    // feeds outputs that are not stored.
+    T w = tile[ty + 1][tx];
+    T e = tile[ty + 1][tx + 2];
+    T n = tile[ty][tx + 1];
+    T s = tile[ty + 2][tx + 1];
+    if (xg == 0) w = c;
+    if (xg == nx - 1) e = c;
+    if (yg == 0) n = c;
+    if (yg == ny - 1) s = c;
+    const T v = point(k, c, w, e, s, n, b, t);
+    if (xg < nx && yg < ny) dst[(size_t)z * xy + (size_t)yg * nx + xg] = v;
+    __syncthreads();
+    b = c;
+    c = t;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+namespace {
+
+const TmaVariant kTmaVariants[kNumTmaVariants] = {
+    {16, 4}, {8, 4}, {16, 6}, {32, 4}, {8, 8}};
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
+                                  void*, const cuuint64_t*, const cuuint64_t*,
+                                  const cuuint32_t*, const cuuint32_t*,
+                                  CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p,
+                                cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+template <typename T>
+Coef<T> load_coef(const void* c) {
+  const T* p = static_cast<const T*>(c);
+  return Coef<T>{p[0], p[1], p[2], p[3], p[4], p[5], p[6]};
+}
+
+int num_sms() {
+  int dev = 0, n = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n > 0 ? n : 1;
+}
+
+// z-chunk so that all CTAs of one step are resident at once (one wave),
+// with chunks of at least `min_chunk` planes.
+int pick_zchunk(int nz, long tiles, int ctas_per_sm, int min_chunk) {
+  long capacity = (long)num_sms() * std::max(ctas_per_sm, 1);
+  long zs = std::max(1L, capacity / std::max(tiles, 1L));
+  zs = std::min<long>(zs, std::max(1, nz / min_chunk));
+  return (int)((nz + zs - 1) / zs);
+}
+
+template <typename T, int BY, int S>
+cudaError_t launch_tma_t(const CUtensorMap& src, void* f2, int nx, int ny,
+                         int nz, const void* coef, int zchunk_override,
+                         cudaStream_t stream, unsigned* dev_err,
+                         LaunchInfo* info) {
+  using C = StepTmaCfg<T, BY, S>;
+  auto kern = step_tma_kernel<T, BY, S>;
+  static bool attr_set = false;  // per instantiation; same on every device
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(
+        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, C::THREADS,
+                                                C::SMEM);
+  const int gx = (nx + C::BX - 1) / C::BX;
+  const int gy = (ny + BY - 1) / BY;
+  const int zchunk = zchunk_override > 0
+                         ? zchunk_override
+                         : pick_zchunk(nz, (long)gx * gy, occ, 8);
+  const int gz = (nz + zchunk - 1) / zchunk;
+  if (info) *info = LaunchInfo{gx, gy, gz, C::THREADS, C::SMEM, zchunk, occ};
+  kern<<<dim3(gx, gy, gz), C::THREADS, C::SMEM, stream>>>(
+      src, static_cast<T*>(f2), nx, ny, nz, load_coef<T>(coef), zchunk,
+      dev_err);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_tma_dtype(const CUtensorMap& src, void* f2, int nx, int ny,
+                             int nz, const void* coef, int variant,
+                             int zchunk_override, cudaStream_t stream,
+                             unsigned* dev_err, LaunchInfo* info) {
+  switch (variant) {
+    case 0: return launch_tma_t<T, 16, 4>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
+    case 1: return launch_tma_t<T, 8, 4>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
+    case 2: return launch_tma_t<T, 16, 6>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
+    case 3: return launch_tma_t<T, 32, 4>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
+    case 4: return launch_tma_t<T, 8, 8>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace
+
+const TmaVariant& tma_variant(int i) { return kTmaVariants[i]; }
+
+int tma_box_x(int dtype) {
+  const int v = 16 / (int)dtype_size(dtype);
+  return 32 * v + 2 * v;
+}
+int tma_box_y(int variant) { return kTmaVariants[variant].by + 2; }
+
+bool tma_eligible(const void* ptr, int nx, int ny, int dtype) {
+  const size_t es = dtype_size(dtype);
+  if ((reinterpret_cast<uintptr_t>(ptr) & 15) != 0) return false;
+  if (((size_t)nx * es) % 16 != 0) return false;  // row pitch, 16-byte rule
+  (void)ny;
+  return encode_fn() != nullptr;
+}
+
+cudaError_t encode_field_map(CUtensorMap* map, const void* ptr, int nx, int ny,
+                             int nz, int dtype, int box_x, int box_y) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return cudaErrorNotSupported;
+  const size_t es = dtype_size(dtype);
+  cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+  cuuint64_t strides[2] = {(cuuint64_t)nx * es, (cuuint64_t)nx * ny * es};
+  cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)box_y, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(map,
+                  dtype == kF64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                  3, const_cast<void*>(ptr), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+cudaError_t launch_step_tma(const CUtensorMap& src, void* f2, int nx, int ny,
+                            int nz, const void* coef, int dtype, int variant,
+                            int zchunk_override, cudaStream_t stream,
+                            unsigned* dev_err, LaunchInfo* info) {
+  if (dtype == kF64)
+    return launch_tma_dtype<double>(src, f2, nx, ny, nz, coef, variant,
+                                    zchunk_override, stream, dev_err, info);
+  return launch_tma_dtype<float>(src, f2, nx, ny, nz, coef, variant,
+                                 zchunk_override, stream, dev_err, info);
+}
+
+cudaError_t launch_step_generic(const void* f1, void* f2, int nx, int ny,
+                                int nz, const void* coef, int dtype,
+                                cudaStream_t stream, LaunchInfo* info) {
+  const int gx = (nx + kGenBX - 1) / kGenBX;
+  const int gy = (ny + kGenBY - 1) / kGenBY;
+  const int zchunk = pick_zchunk(nz, (long)gx * gy, 8, 8);
+  const int gz = (nz + zchunk - 1) / zchunk;
+  if (info) *info = LaunchInfo{gx, gy, gz, kGenBX * kGenBY, 0, zchunk, 8};
+  dim3 grid(gx, gy, gz), block(kGenBX, kGenBY);
+  if (dtype == kF64)
+    step_generic_kernel<double><<<grid, block, 0, stream>>>(
+        static_cast<const double*>(f1), static_cast<double*>(f2), nx, ny, nz,
+        load_coef<double>(coef), zchunk);
+  else
+    step_generic_kernel<float><<<grid, block, 0, stream>>>(
+        static_cast<const float*>(f1), static_cast<float*>(f2), nx, ny, nz,
+        load_coef<float>(coef), zchunk);
+  return cudaGetLastError();
+}
+
+}  // namespace d3d

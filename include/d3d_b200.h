@@ -1,0 +1,143 @@
+/*
+ * d3d_b200.h -- C ABI of libd3d_b200.so, the B200 (sm_100a) backend of the
+ * diffusion3d 7-point stencil.
+ *
+ * This is the boundary a Diffusion3DB200 subclass of the reference's
+ * diffusion3d::Baseline (src/diffusion3d/baseline.h:8-22) binds: plain C,
+ * plain pointers and sizes, no CUDA or C++ types in any signature
+ * (streams are passed as `void*` holding a cudaStream_t; NULL = default
+ * stream).  Each entry point names the reference code it replaces.
+ *
+ * Conventions
+ *  - Fields are x-fastest, offset(i,j,k) = i + j*nx + k*nx*ny, no padding
+ *    (the reference's OFFSET3D, src/diffusion3d/diffusion3d.h:33-34).
+ *  - `coeff` points at 7 values of the plan's dtype in the reference's
+ *    member order ce, cw, cn, cs, ct, cb, cc (diffusion3d.h:52).
+ *  - Every entry returns an int status: D3D_OK (0) or a negative D3D_E_*.
+ *    d3d_last_error() gives the text of the calling thread's last failure.
+ *    The reference's own convention is assert/exit (diffusion3d_cuda.cu:6-9);
+ *    nothing here aborts the process.
+ *  - Results are bit-identical to the reference's Diffusion3DOpenMP for
+ *    FP32 (same operation order, no FMA contraction).
+ *  - A plan is not thread-safe; use one plan per host thread.
+ */
+#ifndef D3D_B200_H_
+#define D3D_B200_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  D3D_OK = 0,
+  D3D_E_INVALID = -1,     /* bad dimensions, pointer or argument */
+  D3D_E_CUDA = -2,        /* a CUDA runtime call failed */
+  D3D_E_OOM = -3,         /* device or pinned allocation failed */
+  D3D_E_TIMEOUT = -4,     /* a bounded device wait ran out */
+  D3D_E_UNSUPPORTED = -5, /* shape/dtype/kernel combination not supported */
+  D3D_E_BUSY = -6         /* admission refused (serving) */
+};
+
+enum { D3D_F32 = 0, D3D_F64 = 1 };
+
+enum {
+  D3D_KERNEL_AUTO = 0,    /* TMA z-march when eligible, else generic */
+  D3D_KERNEL_GENERIC = 1, /* any shape / alignment */
+  D3D_KERNEL_TMA = 2,     /* TMA-staged z-march (row pitch % 16 B == 0) */
+  D3D_KERNEL_TB = 3       /* temporal blocking: tb_depth fused steps/pass */
+};
+
+typedef struct d3d_plan_s* d3d_plan;
+
+/* Library version string. */
+const char* d3d_version(void);
+
+/* Text of the calling thread's most recent failure ("" if none). */
+const char* d3d_last_error(void);
+
+/* Number of kernels this library has launched in this process. */
+unsigned long long d3d_launch_count(void);
+
+/* The coefficients and geometry the reference constructor derives for an
+ * nx*ny*nz grid (Diffusion3D::Diffusion3D, diffusion3d.h:54-66), in the
+ * plan dtype: coeff7 = ce,cw,cn,cs,ct,cb,cc; geom8 = kappa,dx,dy,dz,kx,ky,kz,dt.
+ * Either output may be NULL. */
+int d3d_coefficients(int nx, int ny, int nz, int dtype, void* coeff7,
+                     void* geom8);
+
+/* Creates a plan for one grid shape and precision: the launch
+ * configuration the reference keeps in Diffusion3DCUDA (block_x_, block_y_,
+ * grid_z_; diffusion3d_cuda.h:44-47).  kernel = D3D_KERNEL_*; tb_depth is
+ * the fused step count for D3D_KERNEL_TB (2..4), ignored otherwise.
+ * The plan binds to the CUDA device current at creation. */
+int d3d_plan_create(int nx, int ny, int nz, int dtype, int kernel,
+                    int tb_depth, d3d_plan* out);
+
+/* Overrides the tile variant (0..D3D_NUM_TILE_VARIANTS-1) and z-chunk
+ * (planes per CTA, 0 = automatic) of a plan; used by the autotuner. */
+#define D3D_NUM_TILE_VARIANTS 5
+int d3d_plan_set_tile(d3d_plan plan, int variant, int zchunk);
+
+int d3d_plan_destroy(d3d_plan plan);
+
+/* JSON description of the plan and its last launch geometry. */
+int d3d_plan_info(d3d_plan plan, char* buf, size_t len);
+
+/* Device / pinned-host memory, as Diffusion3DCUDA::InitializeBenchmark and
+ * FinalizeBenchmark use cudaMalloc / cudaMallocHost / cudaFree
+ * (diffusion3d_cuda.cu:329-350). */
+int d3d_device_alloc(size_t bytes, void** ptr);
+int d3d_device_free(void* ptr);
+int d3d_host_alloc(size_t bytes, void** ptr);
+int d3d_host_free(void* ptr);
+int d3d_memcpy(void* dst, const void* src, size_t bytes, void* stream);
+int d3d_stream_sync(void* stream);
+
+/* One time step f2 = stencil(f1) on device buffers: one launch of
+ * diffusion_kernel (diffusion3d_cuda.cu:13-45, launched at :362-363).
+ * f1 and f2 must not overlap. */
+int d3d_step(d3d_plan plan, const void* f1, void* f2, const void* coeff,
+             void* stream);
+
+/* `count` time steps ping-ponging between two device buffers: the launch
+ * loop of Diffusion3DCUDA::RunKernel (diffusion3d_cuda.cu:361-367).  Like
+ * the reference, the buffer pointers are swapped after every step, so on
+ * return *f1 points at the result and *f2 at the other buffer.  With
+ * D3D_KERNEL_TB, count/tb_depth fused passes run first and count%tb_depth
+ * single steps finish the job (exactly `count` steps for any count). */
+int d3d_run(d3d_plan plan, void** f1, void** f2, const void* coeff, int count,
+            void* stream);
+
+/* Diffusion3DCUDA::RunKernel(count) as a whole (diffusion3d_cuda.cu:353-371):
+ * copies host_f1 to dev_f1, runs `count` steps between dev_f1 and dev_f2,
+ * copies the result back into host_f1 and synchronises.  *kernel_ms (may be
+ * NULL) receives the device time of the step loop alone (the reference's
+ * "Kernel-only performance", :373-384). */
+int d3d_run_host(d3d_plan plan, void* host_f1, void* dev_f1, void* dev_f2,
+                 const void* coeff, int count, void* stream, float* kernel_ms);
+
+/* The analytic solution at `time` (GetCorrectAnswer, diffusion3d.h:113-120,
+ * with Initialize, diffusion3d.cc:14-39) written to a device buffer of the
+ * plan dtype, evaluated in double precision on the device. */
+int d3d_analytic(d3d_plan plan, void* out, double time, void* stream);
+
+/* Error norms of device field a against device field b (n elements, any
+ * dtype pair), accumulated in double on the device: out[0] = rms(a-b),
+ * out[1] = max|a-b|, out[2] = max|a-b|/|b|, out[3] = sum(a).  The FP64
+ * counterpart of Baseline::GetAccuracy (baseline.cc:51-60).  Synchronises
+ * `stream`.  Uses plan-owned device scratch. */
+int d3d_compare(d3d_plan plan, const void* a, int a_dtype, const void* b,
+                int b_dtype, size_t n, double out[4], void* stream);
+
+/* Reads and clears the device error word that kernels set instead of
+ * trapping when a bounded wait runs out; returns D3D_E_TIMEOUT if any bit
+ * was set.  Synchronises the current device. */
+int d3d_check_device_errors(unsigned* flags_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* D3D_B200_H_ */

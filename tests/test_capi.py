@@ -1,0 +1,58 @@
+"""C-ABI checks that need no GPU: the library loads, exports every symbol
+include/d3d_b200.h declares, and its host-only entry points behave."""
+import ctypes
+import subprocess
+
+import numpy as np
+import pytest
+
+import benchmarks_b200 as B
+import oracle as O
+
+
+def test_library_loads_and_exports_declared_symbols():
+    L = B.lib()
+    declared = B.declared_symbols()
+    assert len(declared) >= 20
+    for name in declared:
+        assert hasattr(L, name), name
+    # and nothing exported under d3d_ that the header does not declare
+    out = subprocess.run(["nm", "-D", "--defined-only", B.LIB_PATH],
+                         capture_output=True, text=True, check=True).stdout
+    exported = sorted({ln.split()[-1] for ln in out.splitlines()
+                       if ln.split() and ln.split()[-1].startswith("d3d_")})
+    assert exported == declared
+
+
+def test_version_and_last_error():
+    assert "sm_100a" in B.version()
+    rc = B.lib().d3d_coefficients(0, 4, 4, B.F32, None, None)
+    assert rc == B.D3D_E_INVALID
+    assert "bad dims" in B.lib().d3d_last_error().decode()
+
+
+@pytest.mark.parametrize("dims", [(64, 64, 64), (17, 23, 5), (512, 512, 512),
+                                  (24, 40, 16), (1, 1, 1), (96, 16, 33)])
+def test_coefficients_match_oracle(dims):
+    for dt, npdt in ((B.F32, np.float32), (B.F64, np.float64)):
+        c, g = B.coefficients(*dims, dtype=dt)
+        oc, og = O.params(*dims, dtype=npdt)
+        assert c.tobytes() == oc.tobytes()
+        assert g.tobytes() == og.tobytes()
+
+
+def test_plan_create_rejects_bad_arguments():
+    h = ctypes.c_void_p()
+    L = B.lib()
+    assert L.d3d_plan_create(0, 1, 1, B.F32, 0, 1, ctypes.byref(h)) \
+        == B.D3D_E_INVALID
+    assert L.d3d_plan_create(4, 4, 4, 7, 0, 1, ctypes.byref(h)) \
+        == B.D3D_E_INVALID
+    assert L.d3d_plan_create(4, 4, 4, B.F32, 9, 1, ctypes.byref(h)) \
+        == B.D3D_E_INVALID
+    assert L.d3d_plan_create(4, 4, 4, B.F32, B.KERNEL_TB, 7,
+                             ctypes.byref(h)) == B.D3D_E_UNSUPPORTED
+    assert L.d3d_plan_create(1 << 16, 1 << 16, 1, B.F32, 0, 1,
+                             ctypes.byref(h)) == B.D3D_E_INVALID
+    assert L.d3d_step(None, None, None, None, None) == B.D3D_E_INVALID
+    assert L.d3d_run(None, None, None, None, 1, None) == B.D3D_E_INVALID

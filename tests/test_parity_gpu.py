@@ -1,0 +1,240 @@
+"""GPU parity: every kernel, through the C ABI, against the oracle.
+
+FP32 results must be bit-identical to the reference's Diffusion3DOpenMP
+(tests/golden, generated from the reference's own objects, and the pinned
+oracle for other shapes); FP64 results bit-identical to the FP64
+restatement.  At full sizes, where the CPU oracle is too slow, kernels are
+checked against each other (a size-independent property: every kernel
+computes the same bits).
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+import benchmarks_b200 as B
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+ALL_KERNELS = [(B.KERNEL_GENERIC, 1), (B.KERNEL_AUTO, 1), (B.KERNEL_TB, 2),
+               (B.KERNEL_TB, 3), (B.KERNEL_TB, 4)]
+
+
+def _sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def gpu_run(field, coeff, count, kernel=B.KERNEL_AUTO, tb=1, variant=None,
+            zchunk=0):
+    field = np.ascontiguousarray(field)
+    dtype = B.F64 if field.dtype == np.float64 else B.F32
+    nz, ny, nx = field.shape
+    plan = B.Plan(nx, ny, nz, dtype, kernel, tb, variant=variant,
+                  zchunk=zchunk)
+    f1 = torch.from_numpy(field).cuda()
+    f2 = torch.empty_like(f1)
+    res, _ = plan.run(f1, f2, count, coeff)
+    torch.cuda.synchronize()
+    assert B.check_device_errors() == 0
+    out = res.cpu().numpy()
+    plan.close()
+    return out
+
+
+def bits_equal(a, b):
+    return a.dtype == b.dtype and a.tobytes() == b.tobytes()
+
+
+def _coeff(case):
+    return np.array(case["coeff_hex"], np.uint32).view(np.float32)
+
+
+def _case_input(case, fields):
+    key = case["name"] + "/in"
+    if key in fields:
+        return fields[key]
+    f = O.initialize(case["nx"], case["ny"], case["nz"])
+    if case["noise_seed"] is not None:
+        f = f + O.seeded_noise(f.shape, case["noise_seed"])
+    return f
+
+
+@pytest.mark.parametrize("kernel,tb", ALL_KERNELS)
+def test_golden_small_cases_bit_exact(golden, kernel, tb):
+    meta, fields = golden
+    for case in meta["cases"]:
+        if case["name"] + "/out" not in fields:
+            continue
+        out = gpu_run(fields[case["name"] + "/in"], _coeff(case),
+                      case["count"], kernel, tb)
+        assert bits_equal(out, fields[case["name"] + "/out"]), case["name"]
+
+
+@pytest.mark.parametrize("kernel,tb", ALL_KERNELS)
+@pytest.mark.parametrize("name", ["c64_n100", "c128_n100", "c256_n100",
+                                  "c128_n1000_noise"])
+def test_golden_reference_configs_bit_exact(golden, kernel, tb, name):
+    """The reference's own runs (64^3/100, 128^3/100, 256^3/100 and a
+    1000-step noisy 128^3 run): same sha256 of the output bytes, same
+    GetAccuracy."""
+    meta, fields = golden
+    case = {c["name"]: c for c in meta["cases"]}[name]
+    out = gpu_run(_case_input(case, fields), _coeff(case), case["count"],
+                  kernel, tb)
+    assert _sha(out) == case["sha256_out"]
+    acc = O.accuracy(out, case["count"])
+    assert np.float32(acc) == np.float32(case["accuracy"])
+
+
+SHAPES = [(1, 1, 1), (4, 1, 1), (1, 5, 3), (8, 8, 1), (8, 8, 2), (16, 3, 7),
+          (33, 17, 9), (36, 20, 11), (128, 9, 5), (132, 18, 12),
+          (260, 33, 6), (64, 130, 3), (7, 300, 4)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("kernel,tb", ALL_KERNELS)
+def test_ragged_shapes_vs_oracle(shape, kernel, tb):
+    nx, ny, nz = shape
+    c, _ = O.params(nx, ny, nz)
+    fin = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), 21)
+    for count in (0, 1, 5):
+        ref = O.run(fin, c, count)
+        out = gpu_run(fin, c, count, kernel, tb)
+        assert bits_equal(out, ref), (shape, count)
+
+
+@pytest.mark.parametrize("kernel,tb", ALL_KERNELS)
+def test_anisotropic_coefficients(kernel, tb):
+    nx, ny, nz = 44, 27, 19
+    c = np.array([0.11, 0.07, 0.09, 0.13, 0.05, 0.08, 0.47], np.float32)
+    fin = O.seeded_noise((nz, ny, nx), 5, amplitude=1.0)
+    out = gpu_run(fin, c, 9, kernel, tb)
+    assert bits_equal(out, O.run(fin, c, 9))
+
+
+@pytest.mark.parametrize("kernel,tb", ALL_KERNELS)
+@pytest.mark.parametrize("shape", [(20, 12, 9), (64, 64, 64), (36, 5, 40)])
+def test_fp64_bit_exact_vs_fp64_oracle(kernel, tb, shape):
+    nx, ny, nz = shape
+    c, _ = O.params(nx, ny, nz, np.float64)
+    fin = O.initialize(nx, ny, nz, dtype=np.float64)
+    fin = fin + O.seeded_noise(fin.shape, 3).astype(np.float64)
+    out = gpu_run(fin, c, 7, kernel, tb)
+    assert bits_equal(out, O.run(fin, c, 7))
+
+
+@pytest.mark.parametrize("variant", range(B.NUM_TILE_VARIANTS))
+@pytest.mark.parametrize("zchunk", [0, 1, 5, 64])
+def test_tile_variants_and_zchunks(variant, zchunk):
+    nx, ny, nz = 136, 40, 23
+    c, _ = O.params(nx, ny, nz)
+    fin = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), 8)
+    ref = O.run(fin, c, 3)
+    out = gpu_run(fin, c, 3, B.KERNEL_TMA, 1, variant=variant, zchunk=zchunk)
+    assert bits_equal(out, ref)
+
+
+@pytest.mark.parametrize("k", [2, 3, 4])
+@pytest.mark.parametrize("zchunk", [1, 3, 7])
+def test_temporal_blocking_short_chunks(k, zchunk):
+    nx, ny, nz = 64, 24, 21
+    c, _ = O.params(nx, ny, nz)
+    fin = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), 9)
+    for count in (k, 2 * k + 1):
+        out = gpu_run(fin, c, count, B.KERNEL_TB, k, zchunk=zchunk)
+        assert bits_equal(out, O.run(fin, c, count)), count
+
+
+def test_tma_rejects_ineligible_and_auto_falls_to_generic():
+    nx, ny, nz = 17, 8, 4  # row pitch 68 B: not a multiple of 16
+    plan = B.Plan(nx, ny, nz, B.F32, B.KERNEL_TMA)
+    f1 = torch.rand((nz, ny, nx), device="cuda")
+    f2 = torch.empty_like(f1)
+    with pytest.raises(B.D3DError) as ei:
+        plan.step(f1, f2)
+    assert ei.value.code == B.D3D_E_UNSUPPORTED
+    # misaligned base pointer: AUTO still runs (generic kernel), same bits
+    nx = 64
+    c, _ = O.params(nx, ny, nz)
+    fin = O.seeded_noise((nz, ny, nx), 4, amplitude=1.0)
+    big = torch.zeros(fin.size + 1, device="cuda")
+    big[1:] = torch.from_numpy(fin.reshape(-1)).cuda()
+    f1 = big[1:].view(nz, ny, nx)
+    f2 = torch.empty_like(f1)
+    plan = B.Plan(nx, ny, nz, B.F32, B.KERNEL_AUTO)
+    plan.step(f1, f2, c)
+    assert plan.info()["last_kernel"] == "step_generic"
+    assert bits_equal(f2.cpu().numpy(), O.run(fin, c, 1))
+
+
+def test_run_host_matches_device_run():
+    nx, ny, nz = 96, 64, 48
+    c, _ = O.params(nx, ny, nz)
+    fin = O.initialize(nx, ny, nz)
+    plan = B.Plan(nx, ny, nz)
+    host = B.pinned_empty((nz, ny, nx))
+    host[...] = fin
+    f1 = plan.empty()
+    f2 = plan.empty()
+    ms = plan.run_host(host, f1, f2, 11, c)
+    assert ms > 0
+    assert bits_equal(host, O.run(fin, c, 11))
+
+
+def test_full_size_512_kernels_agree():
+    """512^3: every kernel produces the same bits (TMA z-march, generic,
+    temporal blocking k=2,3,4) over 12 steps, and the FP64 device norm
+    between them is exactly zero."""
+    n = 512
+    c, _ = O.params(n, n, n)
+    gen = torch.Generator(device="cuda").manual_seed(1234)
+    base = torch.rand((n, n, n), device="cuda", generator=gen)
+    outs = {}
+    for kernel, tb in ALL_KERNELS:
+        plan = B.Plan(n, n, n, B.F32, kernel, tb)
+        f1 = base.clone()
+        f2 = torch.empty_like(f1)
+        res, _ = plan.run(f1, f2, 12, c)
+        torch.cuda.synchronize()
+        outs[(kernel, tb)] = res
+        del f2
+    ref = outs[(B.KERNEL_AUTO, 1)]
+    plan = B.Plan(n, n, n)
+    for key, v in outs.items():
+        assert torch.equal(v, ref), key
+        nrm = plan.compare(v, ref)
+        assert nrm[0] == 0.0 and nrm[1] == 0.0
+    assert B.check_device_errors() == 0
+
+
+def test_device_compare_matches_oracle_norms():
+    a = O.seeded_noise((40, 30, 20), 1, amplitude=1.0) + np.float32(0.5)
+    b = a + O.seeded_noise(a.shape, 2, amplitude=1e-3)
+    plan = B.Plan(20, 30, 40)
+    got = plan.compare(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda())
+    exp = O.norms(a, b)
+    np.testing.assert_allclose(got, exp, rtol=1e-12, atol=0)
+
+
+def test_device_analytic_close_to_reference_initialize():
+    nx, ny, nz = 64, 48, 40
+    plan = B.Plan(nx, ny, nz, B.F64)
+    out = plan.empty()
+    _, g = O.params(nx, ny, nz, np.float64)
+    t = 37 * g[7]
+    plan.analytic(out, t)
+    ref = O.initialize(nx, ny, nz, time=t, dtype=np.float64)
+    # 1 - a*cos(theta) cancels near the origin; libm and CUDA cos may differ
+    # by an ulp, which the cancellation magnifies to ~1e-13 relative.
+    np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=1e-11, atol=1e-15)
+    # The FP32 analytic field agrees with the reference's own float
+    # Initialize to float rounding.
+    plan32 = B.Plan(nx, ny, nz, B.F32)
+    o32 = plan32.empty()
+    _, g32 = O.params(nx, ny, nz)
+    plan32.analytic(o32, float(np.float32(37) * g32[7]))
+    ref32 = O.initialize(nx, ny, nz, time=np.float32(37) * g32[7])
+    np.testing.assert_allclose(o32.cpu().numpy(), ref32, rtol=1e-5, atol=1e-7)
