@@ -41,6 +41,7 @@ _SIGNATURES = {
     "d3d_coefficients": ([_i, _i, _i, _i, _vp, _vp], _i),
     "d3d_plan_create": ([_i, _i, _i, _i, _i, _i, _vpp], _i),
     "d3d_plan_set_tile": ([_vp, _i, _i], _i),
+    "d3d_plan_set_graphs": ([_vp, _i], _i),
     "d3d_plan_destroy": ([_vp], _i),
     "d3d_plan_info": ([_vp, ctypes.c_char_p, _sz], _i),
     "d3d_device_alloc": ([_sz, _vpp], _i),
@@ -165,6 +166,9 @@ class Plan:
 
     def set_tile(self, variant, zchunk=0):
         check(lib().d3d_plan_set_tile(self._h, variant, zchunk))
+
+    def set_graphs(self, enable: bool):
+        check(lib().d3d_plan_set_graphs(self._h, 1 if enable else 0))
 
     def info(self) -> dict:
         import json

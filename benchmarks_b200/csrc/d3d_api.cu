@@ -116,6 +116,21 @@ struct d3d_plan_s {
   int map_next;
   double* cmp_scratch;  // device scratch for d3d_compare
   cudaEvent_t ev[2];
+  // Step loops captured once into CUDA graphs and replayed, keyed by
+  // buffers, step count, tile choice and coefficient bytes.
+  struct GraphEntry {
+    const void* f1;
+    const void* f2;
+    int count, variant, zchunk;
+    unsigned char coeff[7 * 8];
+    cudaGraphExec_t exec;
+    void* result;
+    void* other;
+    unsigned long long launches;
+  } graphs[4];
+  int graph_next;
+  int use_graphs;
+  cudaStream_t capture_stream;
   d3d::LaunchInfo last;
   const char* last_kernel;
 };
@@ -218,6 +233,83 @@ int run_loop(d3d_plan p, void** f1, void** f2, const void* coeff, int count,
   return D3D_OK;
 }
 
+void drop_graphs(d3d_plan p) {
+  for (auto& g : p->graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+  }
+}
+
+// run_loop through a cached CUDA graph: the `count` launches of a
+// RunKernel-style loop are captured once and replayed as one graph launch,
+// which removes the per-launch host overhead and the gaps between steps.
+// Falls back to direct launches when the caller's stream is itself being
+// captured (the launches then land in the caller's graph).
+int run_graphed(d3d_plan p, void** f1, void** f2, const void* coeff,
+                int count, cudaStream_t s) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (!p->use_graphs || count < 2 ||
+      cudaStreamIsCapturing(s, &cap) != cudaSuccess ||
+      cap != cudaStreamCaptureStatusNone)
+    return run_loop(p, f1, f2, coeff, count, s);
+  const size_t cb = 7 * d3d::dtype_size(p->dtype);
+  d3d_plan_s::GraphEntry* hit = nullptr;
+  for (auto& g : p->graphs)
+    if (g.exec && g.f1 == *f1 && g.f2 == *f2 && g.count == count &&
+        g.variant == p->variant && g.zchunk == p->zchunk &&
+        memcmp(g.coeff, coeff, cb) == 0) {
+      hit = &g;
+      break;
+    }
+  if (!hit) {
+    if (!p->capture_stream)
+      D3D_TRY(cudaStreamCreateWithFlags(&p->capture_stream,
+                                        cudaStreamNonBlocking),
+              "cudaStreamCreateWithFlags");
+    auto& g = p->graphs[p->graph_next];
+    p->graph_next = (p->graph_next + 1) % 4;
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+    void* a = *f1;
+    void* b = *f2;
+    const unsigned long long l0 = g_launches.load();
+    D3D_TRY(cudaStreamBeginCapture(p->capture_stream,
+                                   cudaStreamCaptureModeThreadLocal),
+            "cudaStreamBeginCapture");
+    int rc = run_loop(p, &a, &b, coeff, count, p->capture_stream);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(p->capture_stream, &graph);
+    const unsigned long long captured = g_launches.load() - l0;
+    g_launches.fetch_sub(captured);  // counted when the graph runs
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      g.exec = nullptr;
+      return cuda_fail(e, "cudaGraphInstantiate");
+    }
+    g.f1 = *f1;
+    g.f2 = *f2;
+    g.count = count;
+    g.variant = p->variant;
+    g.zchunk = p->zchunk;
+    memcpy(g.coeff, coeff, cb);
+    g.result = a;
+    g.other = b;
+    g.launches = captured;
+    hit = &g;
+  }
+  D3D_TRY(cudaGraphLaunch(hit->exec, s), "cudaGraphLaunch");
+  g_launches.fetch_add(hit->launches, std::memory_order_relaxed);
+  *f1 = hit->result;
+  *f2 = hit->other;
+  return D3D_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -271,6 +363,7 @@ int d3d_plan_create(int nx, int ny, int nz, int dtype, int kernel,
   p->device = dev;
   p->n = (size_t)nx * ny * nz;
   p->last_kernel = "";
+  p->use_graphs = 1;
   for (auto& m : p->maps) m.ptr = nullptr;
   cudaError_t e = cudaEventCreate(&p->ev[0]);
   if (e == cudaSuccess) e = cudaEventCreate(&p->ev[1]);
@@ -293,12 +386,21 @@ int d3d_plan_set_tile(d3d_plan p, int variant, int zchunk) {
   return D3D_OK;
 }
 
+int d3d_plan_set_graphs(d3d_plan p, int enable) {
+  if (!p) return fail(D3D_E_INVALID, "plan is NULL");
+  p->use_graphs = enable ? 1 : 0;
+  if (!enable) drop_graphs(p);
+  return D3D_OK;
+}
+
 int d3d_plan_destroy(d3d_plan p) {
   if (!p) return D3D_OK;
   int prev = -1;
   cudaGetDevice(&prev);
   if (prev != p->device) cudaSetDevice(p->device);
   if (p->cmp_scratch) cudaFree(p->cmp_scratch);
+  drop_graphs(p);
+  if (p->capture_stream) cudaStreamDestroy(p->capture_stream);
   cudaEventDestroy(p->ev[0]);
   cudaEventDestroy(p->ev[1]);
   if (prev >= 0 && prev != p->device) cudaSetDevice(prev);
@@ -314,11 +416,11 @@ int d3d_plan_info(d3d_plan p, char* buf, size_t len) {
            "\"kernel\": %d, \"tb_depth\": %d, \"variant\": %d, "
            "\"zchunk\": %d, \"device\": %d, \"last_kernel\": \"%s\", "
            "\"grid\": [%d, %d, %d], \"block\": %d, \"smem\": %d, "
-           "\"launch_zchunk\": %d, \"ctas_per_sm\": %d}",
+           "\"launch_zchunk\": %d, \"ctas_per_sm\": %d, \"graphs\": %d}",
            p->nx, p->ny, p->nz, p->dtype == kF64 ? "f64" : "f32", p->kernel,
            p->tb_depth, p->variant, p->zchunk, p->device, p->last_kernel,
            L.grid_x, L.grid_y, L.grid_z, L.block, L.smem_bytes, L.zchunk,
-           L.ctas_per_sm);
+           L.ctas_per_sm, p->use_graphs);
   return D3D_OK;
 }
 
@@ -373,7 +475,7 @@ int d3d_run(d3d_plan p, void** f1, void** f2, const void* coeff, int count,
   if (count < 0) return fail(D3D_E_INVALID, "negative count %d", count);
   int rc = check_device(p);
   if (rc) return rc;
-  return run_loop(p, f1, f2, coeff, count, as_stream(stream));
+  return run_graphed(p, f1, f2, coeff, count, as_stream(stream));
 }
 
 int d3d_run_host(d3d_plan p, void* host_f1, void* dev_f1, void* dev_f2,
@@ -392,7 +494,7 @@ int d3d_run_host(d3d_plan p, void* host_f1, void* dev_f1, void* dev_f2,
   D3D_TRY(cudaEventRecord(p->ev[0], s), "cudaEventRecord");
   void* a = dev_f1;
   void* b = dev_f2;
-  rc = run_loop(p, &a, &b, coeff, count, s);
+  rc = run_graphed(p, &a, &b, coeff, count, s);
   if (rc) return rc;
   D3D_TRY(cudaEventRecord(p->ev[1], s), "cudaEventRecord");
   D3D_TRY(cudaMemcpyAsync(host_f1, a, bytes, cudaMemcpyDeviceToHost, s),

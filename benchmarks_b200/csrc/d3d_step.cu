@@ -56,6 +56,8 @@ __global__ void __launch_bounds__(StepTmaCfg<T, BY, S>::THREADS)
                     T* __restrict__ dst, int nx, int ny, int nz, Coef<T> k,
                     int zchunk, unsigned* __restrict__ dev_err) {
   using C = StepTmaCfg<T, BY, S>;
+  constexpr int V = C::V;
+  constexpr int RPW = C::RPW;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
@@ -74,6 +76,7 @@ __global__ void __launch_bounds__(StepTmaCfg<T, BY, S>::THREADS)
 
   auto stage_of = [&](int p) { return (p - pbase) % S; };
   auto parity_of = [&](int p) { return (unsigned)(((p - pbase) / S) & 1); };
+  auto stage_ptr = [&](int p) { return stages + stage_of(p) * C::STAGE_ELEMS; };
   auto issue = [&](int p) {
     const int s = stage_of(p);
     mbar_arrive_expect_tx(&bars[s], C::STAGE_BYTES_RAW);
@@ -91,13 +94,33 @@ __global__ void __launch_bounds__(StepTmaCfg<T, BY, S>::THREADS)
     for (int p = pbase; p <= plast && p < pbase + S; ++p) issue(p);
   }
 
-  const int xg = x0 + C::V * lane;   // first x of this thread's segment
-  const int col = C::HX + C::V * lane;  // its smem column
-  const bool x_lo = (xg == 0);
-  const bool x_hi = (xg + C::V - 1 == nx - 1);
+  // Loop-invariant addressing.  Every replicated-boundary rule becomes an
+  // address: at y = 0 the north load reads the centre row, at y = ny-1 the
+  // south load does, at x = 0 lane 0 reads its own first element as w; at
+  // z = nz-1 the top plane is the centre plane (stage_ptr(min(z+1, nz-1))).
+  const int xg = x0 + V * lane;      // first x of this thread's segment
+  const int col = C::HX + V * lane;  // its shared-memory column
+  const bool x_hi = (xg + V - 1 == nx - 1);
+  int c_off[RPW], n_off[RPW], s_off[RPW];
+  size_t g_off[RPW];
+  bool store_ok[RPW];
+#pragma unroll
+  for (int r = 0; r < RPW; ++r) {
+    const int row = warp * RPW + r;
+    const int yg = y0 + row;
+    c_off[r] = (row + 1) * C::P + col;
+    n_off[r] = (yg == 0) ? c_off[r] : row * C::P + col;
+    s_off[r] = (yg >= ny - 1) ? c_off[r] : (row + 2) * C::P + col;
+    g_off[r] = (size_t)yg * nx + xg;
+    store_ok[r] = (yg < ny) && (xg < nx);
+  }
+  const int wl_adj = (xg == 0) ? 0 : -1;  // lane 0's w load
+  const size_t plane = (size_t)nx * ny;
+  const typename SegCoef<T>::type kk = SegCoef<T>::make(k);
 
-  V16<T> creg[C::RPW], breg[C::RPW];
-  // Planes issued but not yet waited for, drained if a wait runs out.
+  // Register queue: three rotating sets of RPW segments (b, c, t roles),
+  // unrolled three ways so no values are copied between iterations.
+  V16<T> q0[RPW], q1[RPW], q2[RPW];
   int drain_lo = pbase, drain_hi = min(plast, pbase + S - 1);
 
   // Prologue: planes z0 (c) and z0-1 (b), and z0+1 (t of the first step).
@@ -111,61 +134,64 @@ __global__ void __launch_bounds__(StepTmaCfg<T, BY, S>::THREADS)
     goto drain;
   }
   {
-    const T* sc = stages + stage_of(z0) * C::STAGE_ELEMS;
-    const T* sb = stages + stage_of(pbase) * C::STAGE_ELEMS;
+    const T* sc = stage_ptr(z0);
+    const T* sb = stage_ptr(pbase);  // == sc when z0 == 0 (b = c at z = 0)
 #pragma unroll
-    for (int r = 0; r < C::RPW; ++r) {
-      const int row = warp * C::RPW + r;
-      creg[r] = ld16_shared(sc + (row + 1) * C::P + col);
-      breg[r] = (z0 > 0) ? ld16_shared(sb + (row + 1) * C::P + col) : creg[r];
+    for (int r = 0; r < RPW; ++r) {
+      q1[r] = ld16_shared(sc + c_off[r]);
+      q0[r] = ld16_shared(sb + c_off[r]);
     }
   }
   __syncthreads();
   if (z0 > 0 && threadIdx.x == 0 && pbase + S <= plast) issue(pbase + S);
 
-  for (int z = z0; z < z1; ++z) {
-    const bool has_t = (z + 1 < nz);
-    const T* sc = stages + stage_of(z) * C::STAGE_ELEMS;
-    const T* st = stages + stage_of(has_t ? z + 1 : z) * C::STAGE_ELEMS;
-    T* out_plane = dst + (size_t)z * ny * nx;
+  {
+    // One z step: b, c in registers, t loaded into `vt`; then wait for the
+    // next t plane and recycle plane z's stage.  Returns false on timeout.
+    auto step = [&](int z, const V16<T>* vb, const V16<T>* vc,
+                    V16<T>* vt) -> bool {
+      const T* sc = stage_ptr(z);
+      const T* st = stage_ptr(min(z + 1, nz - 1));
+      T* out = dst + (size_t)z * plane;
 #pragma unroll
-    for (int r = 0; r < C::RPW; ++r) {
-      const int row = warp * C::RPW + r;
-      const int yg = y0 + row;
-      const V16<T> c = creg[r];
-      const V16<T> t = has_t ? ld16_shared(st + (row + 1) * C::P + col) : c;
-      const V16<T> n = (yg == 0) ? c : ld16_shared(sc + row * C::P + col);
-      const V16<T> s =
-          (yg == ny - 1) ? c : ld16_shared(sc + (row + 2) * C::P + col);
-      T wl = __shfl_up_sync(0xffffffffu, c.e[C::V - 1], 1);
-      T er = __shfl_down_sync(0xffffffffu, c.e[0], 1);
-      if (lane == 0) wl = sc[(row + 1) * C::P + col - 1];
-      if (lane == 31) er = sc[(row + 1) * C::P + col + C::V];
-      if (x_lo) wl = c.e[0];
-      if (x_hi) er = c.e[C::V - 1];
-      V16<T> o;
-#pragma unroll
-      for (int i = 0; i < C::V; ++i) {
-        const T w = (i == 0) ? wl : c.e[i - 1];
-        const T e = (i == C::V - 1) ? er : c.e[i + 1];
-        o.e[i] = point(k, c.e[i], w, e, s.e[i], n.e[i], breg[r].e[i], t.e[i]);
+      for (int r = 0; r < RPW; ++r) {
+        vt[r] = ld16_shared(st + c_off[r]);
+        const V16<T> n = ld16_shared(sc + n_off[r]);
+        const V16<T> s = ld16_shared(sc + s_off[r]);
+        T wl = __shfl_up_sync(0xffffffffu, vc[r].e[V - 1], 1);
+        T er = __shfl_down_sync(0xffffffffu, vc[r].e[0], 1);
+        if (lane == 0) wl = sc[c_off[r] + wl_adj];
+        if (lane == 31) er = sc[c_off[r] + V];
+        if (x_hi) er = vc[r].e[V - 1];
+        const V16<T> o = point_seg<T>(kk, vc[r], n, s, vb[r], vt[r], wl, er);
+        if (store_ok[r]) st16_global(out + g_off[r], o);
       }
-      if (yg < ny && xg < nx) st16_global(out_plane + (size_t)yg * nx + xg, o);
-      breg[r] = c;
-      creg[r] = t;
+      // Plane z+2 is the t plane of the next step; wait for it before the
+      // barrier that releases plane z's stage to the producer.
+      bool ok2 = true;
+      if (z + 2 <= plast && z + 1 < z1)
+        ok2 = mbar_wait_bounded(&bars[stage_of(z + 2)], parity_of(z + 2));
+      if (!__syncthreads_and(ok2)) {
+        if (threadIdx.x == 0) atomicOr(dev_err, kDevWaitTimeout);
+        return false;
+      }
+      if (threadIdx.x == 0 && z + S <= plast) issue(z + S);
+      return true;
+    };
+
+    int zf = -1;  // the step whose wait ran out
+    for (int z = z0; z < z1; z += 3) {
+      if (!step(z, q0, q1, q2)) { zf = z; break; }
+      if (z + 1 >= z1) break;
+      if (!step(z + 1, q1, q2, q0)) { zf = z + 1; break; }
+      if (z + 2 >= z1) break;
+      if (!step(z + 2, q2, q0, q1)) { zf = z + 2; break; }
     }
-    // Plane z+2 is the t plane of the next step; wait for it before the
-    // barrier that releases plane z's stage to the producer.
-    bool ok2 = true;
-    if (z + 2 <= plast && z + 1 < z1)
-      ok2 = mbar_wait_bounded(&bars[stage_of(z + 2)], parity_of(z + 2));
-    if (!__syncthreads_and(ok2)) {
-      if (threadIdx.x == 0) atomicOr(dev_err, kDevWaitTimeout);
-      drain_lo = z + 2;
-      drain_hi = min(plast, z + S - 1);
+    if (zf >= 0) {
+      drain_lo = zf + 2;
+      drain_hi = min(plast, zf + S - 1);
       goto drain;
     }
-    if (threadIdx.x == 0 && z + S <= plast) issue(z + S);
   }
   return;
 
@@ -275,12 +301,6 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-template <typename T>
-Coef<T> load_coef(const void* c) {
-  const T* p = static_cast<const T*>(c);
-  return Coef<T>{p[0], p[1], p[2], p[3], p[4], p[5], p[6]};
-}
-
 int num_sms() {
   int dev = 0, n = 0;
   cudaGetDevice(&dev);
@@ -322,7 +342,7 @@ cudaError_t launch_tma_t(const CUtensorMap& src, void* f2, int nx, int ny,
   const int gz = (nz + zchunk - 1) / zchunk;
   if (info) *info = LaunchInfo{gx, gy, gz, C::THREADS, C::SMEM, zchunk, occ};
   kern<<<dim3(gx, gy, gz), C::THREADS, C::SMEM, stream>>>(
-      src, static_cast<T*>(f2), nx, ny, nz, load_coef<T>(coef), zchunk,
+      src, static_cast<T*>(f2), nx, ny, nz, coef_from<T>(coef), zchunk,
       dev_err);
   return cudaGetLastError();
 }
@@ -402,11 +422,11 @@ cudaError_t launch_step_generic(const void* f1, void* f2, int nx, int ny,
   if (dtype == kF64)
     step_generic_kernel<double><<<grid, block, 0, stream>>>(
         static_cast<const double*>(f1), static_cast<double*>(f2), nx, ny, nz,
-        load_coef<double>(coef), zchunk);
+        coef_from<double>(coef), zchunk);
   else
     step_generic_kernel<float><<<grid, block, 0, stream>>>(
         static_cast<const float*>(f1), static_cast<float*>(f2), nx, ny, nz,
-        load_coef<float>(coef), zchunk);
+        coef_from<float>(coef), zchunk);
   return cudaGetLastError();
 }
 

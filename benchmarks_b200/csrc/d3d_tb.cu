@@ -7,21 +7,30 @@
 //
 // Per CTA: a BX x BY xy tile, overlapped by a K-cell halo (redundant
 // compute at the edges instead of inter-CTA exchange), marching a z-chunk.
-//   level 0      z-planes of the input, loaded by TMA into an S0-deep ring
-//                of (BX + 2*HX) x (BY + 2K) boxes (mbarrier completion);
-//   level j<K    the field after j steps, 3-plane rings in shared memory,
-//                region shrinking by one cell per level;
-//   level K      written to HBM with 128-bit stores.
-// When level-0 plane q lands, level j computes plane q-j from level j-1's
-// planes q-j-1, q-j, q-j+1 (one __syncthreads between levels).  Plane
-// indices are clamped to [0, nz), which is the reference's replicated
-// z-neighbour; x/y edges select the centre value explicitly (TMA fills
-// out-of-range cells with zeros).  Points outside the domain compute
-// values that no in-domain point ever reads.
+//
+//   level 0   input z-planes, TMA box loads ((BX + 2*HX) x (BY + 2K)) into
+//             an S0-deep shared ring completed through mbarriers;
+//   level j   the field after j steps (1 <= j < K): each thread keeps the
+//             last three planes of its own cells in registers (three sets
+//             whose b/c/t roles rotate with the iteration, so nothing is
+//             copied) and publishes the newest plane to a 2-slot shared
+//             ring for its neighbours;
+//   level K   the output, 128-bit stores to HBM.
+//
+// When level-0 plane q lands, level j computes plane q-j.  It takes b, c, t
+// from its own registers (level 1: from the TMA ring) and n, s, w, e from
+// level j-1's shared plane q-j, which was written in the previous
+// iteration -- so one __syncthreads per plane suffices, whatever K is.
+// The cell->thread assignment is fixed for the CTA's lifetime, which makes
+// every address, and every replicated-boundary rule (an address that reads
+// the centre cell), loop-invariant.  At z the rules are: plane -1 is plane
+// 0 and plane nz is plane nz-1.  Cells outside the domain compute values no
+// in-domain cell ever reads.
 //
 // Each point update is d3d::point, so the fused result is bit-identical to
 // K single steps (and to the reference's CPU loop).
 #include <algorithm>
+#include <type_traits>
 
 #include "d3d_common.cuh"
 #include "d3d_kernels.h"
@@ -39,39 +48,54 @@ struct TbCfg {
   static constexpr int R = BY + 2 * K;               // rows of level 0
   static constexpr int STAGE0_RAW = P * R * (int)sizeof(T);
   static constexpr int STAGE0 = (STAGE0_RAW + 127) / 128 * 128;
-  // Level j (1..K-1) holds rows [j, R-j): R-2j rows, 3 planes.
-  __host__ __device__ static constexpr int level_rows(int j) {
-    return R - 2 * j;
+  static constexpr int STAGE0_ELEMS = STAGE0 / (int)sizeof(T);
+  // Cells each level computes: rows [j, R-j), segments [seg_lo(j), seg_hi(j)].
+  __host__ __device__ static constexpr int seg_lo(int j) {
+    return (HX - (K - j)) / V;
   }
-  __host__ __device__ static constexpr int level_plane_elems(int j) {
-    return level_rows(j) * P;
+  __host__ __device__ static constexpr int seg_hi(int j) {
+    return (HX + BX + (K - j) - 1) / V;
   }
-  __host__ __device__ static constexpr int level_bytes_sum(int upto) {
-    return upto <= 0 ? 0
-                     : level_bytes_sum(upto - 1) +
-                           3 * level_plane_elems(upto) * (int)sizeof(T);
+  // Thread items cover level 1's region (the largest computed one).
+  static constexpr int NS = seg_hi(1) - seg_lo(1) + 1;
+  static constexpr int NR = R - 2;
+  static constexpr int NITEMS = NR * NS;
+  static constexpr int NI = (NITEMS + THREADS - 1) / THREADS;
+  // Level j (1..K-1) shared ring: 2 planes of rows [j, R-j).
+  __host__ __device__ static constexpr int ring_plane(int j) {
+    return (R - 2 * j) * P;
   }
-  static constexpr int LEVELS_BYTES = level_bytes_sum(K - 1);
-  static constexpr int SMEM = S0 * STAGE0 + LEVELS_BYTES + S0 * 8 + 256;
+  __host__ __device__ static constexpr int ring_off(int j) {
+    return j <= 1 ? 0 : ring_off(j - 1) + 2 * ring_plane(j - 1);
+  }
+  static constexpr int RINGS_BYTES = ring_off(K) * (int)sizeof(T);
+  static constexpr int SMEM = S0 * STAGE0 + RINGS_BYTES + S0 * 8 + 256;
+  static constexpr int KM1 = K > 1 ? K - 1 : 1;
+  // K = 2 fits two CTAs per SM in registers without spilling; deeper
+  // fusion keeps three register sets per level and runs one CTA per SM.
+  static constexpr int MIN_CTAS = K == 2 ? 2 : 1;
   static_assert(P <= 256 && R <= 256, "TMA box dimensions are at most 256");
   static_assert(S0 >= 4, "ring holds planes q-2..q plus loads in flight");
+  static_assert(K >= 2 && K <= 4, "fusion depth");
 };
 
 template <typename T, int K, int BY, int S0>
-__global__ void __launch_bounds__(TbCfg<T, K, BY, S0>::THREADS)
+__global__ void __launch_bounds__(TbCfg<T, K, BY, S0>::THREADS,
+                                  TbCfg<T, K, BY, S0>::MIN_CTAS)
     steps_tb_kernel(const __grid_constant__ CUtensorMap src,
                     T* __restrict__ dst, int nx, int ny, int nz, Coef<T> k,
                     int zchunk, unsigned* __restrict__ dev_err) {
   using C = TbCfg<T, K, BY, S0>;
   constexpr int V = C::V;
   constexpr int P = C::P;
+  constexpr int NI = C::NI;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
   T* stage0 = reinterpret_cast<T*>(base);
-  T* levels = reinterpret_cast<T*>(base + S0 * C::STAGE0);
+  T* rings = reinterpret_cast<T*>(base + S0 * C::STAGE0);
   uint64_t* bars =
-      reinterpret_cast<uint64_t*>(base + S0 * C::STAGE0 + C::LEVELS_BYTES);
+      reinterpret_cast<uint64_t*>(base + S0 * C::STAGE0 + C::RINGS_BYTES);
 
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * C::BX;
@@ -86,21 +110,17 @@ __global__ void __launch_bounds__(TbCfg<T, K, BY, S0>::THREADS)
 
   auto stage_of = [&](int p) { return (p - lo0) % S0; };
   auto parity_of = [&](int p) { return (unsigned)(((p - lo0) / S0) & 1); };
+  auto stage_ptr = [&](int p) { return stage0 + stage_of(p) * C::STAGE0_ELEMS; };
   auto issue = [&](int p) {
     const int s = stage_of(p);
     mbar_arrive_expect_tx(&bars[s], C::STAGE0_RAW);
-    tma_load_3d(stage0 + s * (C::STAGE0 / (int)sizeof(T)), &src, &bars[s],
-                x0 - C::HX, y0 - K, p);
+    tma_load_3d(stage0 + s * C::STAGE0_ELEMS, &src, &bars[s], x0 - C::HX,
+                y0 - K, p);
   };
-  // Pointer to row `r` (level-0 row numbering) of level j's plane p.
-  auto row_ptr = [&](int j, int p, int r) -> T* {
-    if (j == 0)
-      return stage0 + stage_of(p) * (C::STAGE0 / (int)sizeof(T)) + r * P;
-    int off = 0;
-#pragma unroll
-    for (int i = 1; i < K; ++i)
-      if (i < j) off += 3 * C::level_plane_elems(i);
-    return levels + off + (p % 3) * C::level_plane_elems(j) + (r - j) * P;
+  // Base of level j's ring slot for plane p, addressed with level-0 row
+  // numbering (row r lives at (r - j) * P).
+  auto ring_ptr = [&](int j, int p) {
+    return rings + C::ring_off(j) + (p & 1) * C::ring_plane(j) - j * P;
   };
 
   if (tid == 0) {
@@ -112,75 +132,131 @@ __global__ void __launch_bounds__(TbCfg<T, K, BY, S0>::THREADS)
   if (tid == 0)
     for (int p = lo0; p <= hi0 && p < lo0 + S0; ++p) issue(p);
 
-  const int qend = z1 - 1 + K;
-  // Planes issued but not yet waited for, drained if a wait runs out.
-  int drain_lo = lo0, drain_hi = -1;
-  for (int q = lo0; q <= qend; ++q) {
-    bool ok = true;
-    if (q <= hi0) ok = mbar_wait_bounded(&bars[stage_of(q)], parity_of(q));
-    if (!__syncthreads_and(ok)) {
-      if (tid == 0) atomicOr(dev_err, kDevWaitTimeout);
-      // Issued so far: the prologue's planes and, from iteration lo0+2 on,
-      // plane q'-2+S0 at each earlier iteration q'.
-      drain_lo = q;
-      drain_hi = min(hi0, max(lo0 + S0 - 1, q - 3 + S0));
-      goto drain;
-    }
+  // Fixed cells of this thread: offsets within a level-0-numbered plane.
+  int c_off[NI], n_off[NI], s_off[NI], w_off[NI], e_off[NI];
+  size_t g_off[NI];
+  unsigned lvmask[NI];  // bit j: the cell is in level j's region
+  bool store_ok[NI];
 #pragma unroll
-    for (int j = 1; j <= K; ++j) {
-      const int p = q - j;
-      if (p >= lo(j) && p <= hi(j)) {
-        const int pb = max(p - 1, 0);       // clamped z-neighbours
-        const int pt = min(p + 1, nz - 1);  // (replicated at the edges)
-        const int zg = p;
-        const int row_lo = j;
-        const int nrows = C::R - 2 * j;
-        const int seg_lo = (C::HX - (K - j)) / V;
-        const int seg_hi = (C::HX + C::BX + (K - j) - 1) / V;
-        const int nseg = seg_hi - seg_lo + 1;
-        const int items = nrows * nseg;
-        for (int it = tid; it < items; it += C::THREADS) {
-          const int r = row_lo + it / nseg;
-          const int col = (seg_lo + it % nseg) * V;
-          const int yg = y0 - K + r;
-          const int xg = x0 - C::HX + col;
-          const T* rc = row_ptr(j - 1, p, r);
-          const V16<T> c = ld16_shared(rc + col);
-          const V16<T> n = ld16_shared(row_ptr(j - 1, p, r - 1) + col);
-          const V16<T> s = ld16_shared(row_ptr(j - 1, p, r + 1) + col);
-          const V16<T> b = ld16_shared(row_ptr(j - 1, pb, r) + col);
-          const V16<T> t = ld16_shared(row_ptr(j - 1, pt, r) + col);
-          const T wl = rc[max(col - 1, 0)];
-          const T er = rc[min(col + V, P - 1)];
-          V16<T> o;
+  for (int i = 0; i < NI; ++i) {
+    const int it = tid + i * C::THREADS;
+    const bool valid = it < C::NITEMS;
+    const int itc = valid ? it : 0;
+    const int r = 1 + itc / C::NS;
+    const int sg = C::seg_lo(1) + itc % C::NS;
+    const int col = sg * V;
+    const int yg = y0 - K + r;
+    const int xg = x0 - C::HX + col;
+    c_off[i] = r * P + col;
+    n_off[i] = (yg == 0 ? r : r - 1) * P + col;
+    s_off[i] = (yg == ny - 1 ? r : r + 1) * P + col;
+    w_off[i] = r * P + (xg == 0 ? col : max(col - 1, 0));
+    e_off[i] = r * P + (xg + V - 1 == nx - 1 ? col + V - 1 : min(col + V, P - 1));
+    g_off[i] = (size_t)(yg < 0 ? 0 : yg) * nx + (xg < 0 ? 0 : xg);
+    unsigned m = 0;
 #pragma unroll
-          for (int i = 0; i < V; ++i) {
-            const int xi = xg + i;
-            const T ci = c.e[i];
-            T w = (i == 0) ? wl : c.e[i - 1];
-            T e = (i == V - 1) ? er : c.e[i + 1];
-            if (xi == 0) w = ci;
-            if (xi == nx - 1) e = ci;
-            const T ni = (yg == 0) ? ci : n.e[i];
-            const T si = (yg == ny - 1) ? ci : s.e[i];
-            o.e[i] = point(k, ci, w, e, si, ni, b.e[i], t.e[i]);
+    for (int j = 1; j <= K; ++j)
+      if (valid && r >= j && r < C::R - j && sg >= C::seg_lo(j) &&
+          sg <= C::seg_hi(j))
+        m |= 1u << j;
+    lvmask[i] = m;
+    store_ok[i] = valid && (m >> K & 1u) && yg < ny && xg < nx;
+  }
+  const size_t plane = (size_t)nx * ny;
+  const typename SegCoef<T>::type kk = SegCoef<T>::make(k);
+
+  // X[set][level-1][item]: three register sets per level whose roles
+  // (b, c, t) rotate with the iteration.
+  V16<T> X[3][C::KM1][NI];
+
+  int drain_lo = lo0, drain_hi = min(hi0, lo0 + S0 - 1);
+  bool ok = mbar_wait_bounded(&bars[stage_of(lo0)], parity_of(lo0));
+  int qf = -1;  // iteration whose wait ran out
+  if (!__syncthreads_and(ok)) {
+    if (tid == 0) atomicOr(dev_err, kDevWaitTimeout);
+    goto drain;
+  }
+
+  {
+    auto iter = [&](auto rot, int q) -> bool {
+      constexpr int RB = (decltype(rot)::value + 0) % 3;
+      constexpr int RC = (decltype(rot)::value + 1) % 3;
+      constexpr int RT = (decltype(rot)::value + 2) % 3;
+#pragma unroll
+      for (int j = 1; j <= K; ++j) {
+        const int p = q - j;
+        if (j >= 2 && p == nz - 1) {
+          // Level j-1 has no plane nz: its t is its own last plane.
+#pragma unroll
+          for (int i = 0; i < NI; ++i)
+            X[RT][max(j - 2, 0)][i] = X[RC][max(j - 2, 0)][i];
+        }
+        if (p < lo(j) || p > hi(j)) continue;
+        const T* cb = (j == 1) ? stage_ptr(p) : ring_ptr(j - 1, p);
+        const T* bb = stage_ptr(max(p - 1, 0));
+        const T* tb = stage_ptr(min(p + 1, nz - 1));
+        T* ob = (j < K) ? ring_ptr(min(j, K - 1), p) : nullptr;
+        T* gb = dst + (size_t)p * plane;
+#pragma unroll
+        for (int i = 0; i < NI; ++i) {
+          if (!(lvmask[i] >> j & 1u)) continue;
+          V16<T> c, b, t;
+          if (j == 1) {
+            c = ld16_shared(cb + c_off[i]);
+            b = ld16_shared(bb + c_off[i]);
+            t = ld16_shared(tb + c_off[i]);
+          } else {
+            c = X[RC][max(j - 2, 0)][i];
+            b = X[RB][max(j - 2, 0)][i];
+            t = X[RT][max(j - 2, 0)][i];
           }
+          const V16<T> n = ld16_shared(cb + n_off[i]);
+          const V16<T> s = ld16_shared(cb + s_off[i]);
+          const T wl = cb[w_off[i]];
+          const T er = cb[e_off[i]];
+          const V16<T> o = point_seg<T>(kk, c, n, s, b, t, wl, er);
           if (j < K) {
-            *reinterpret_cast<V16<T>*>(row_ptr(j, p, r) + col) = o;
-          } else if (yg < ny && xg < nx) {
-            st16_global(dst + ((size_t)zg * ny + yg) * nx + xg, o);
+            X[RT][min(j - 1, C::KM1 - 1)][i] = o;
+            *reinterpret_cast<V16<T>*>(ob + c_off[i]) = o;
+          } else if (store_ok[i]) {
+            st16_global(gb + g_off[i], o);
           }
         }
       }
-      __syncthreads();
-      // After level 1 consumed it, level-0 plane q-2 is free: refill.
-      if (j == 1 && tid == 0) {
-        const int pf = q - 2;
-        if (pf >= lo0 && pf + S0 <= hi0) issue(pf + S0);
+      // Plane -1 is plane 0: the level that just produced plane 0 also
+      // supplies it as the b plane of its next consumer.
+#pragma unroll
+      for (int L = 1; L < K; ++L)
+        if (q - L == 0) {
+#pragma unroll
+          for (int i = 0; i < NI; ++i) X[RC][L - 1][i] = X[RT][L - 1][i];
+        }
+      // Level 1 of the next iteration reads level-0 planes q-1..q+1.
+      bool ok2 = true;
+      if (q + 1 <= hi0)
+        ok2 = mbar_wait_bounded(&bars[stage_of(q + 1)], parity_of(q + 1));
+      if (!__syncthreads_and(ok2)) {
+        if (tid == 0) atomicOr(dev_err, kDevWaitTimeout);
+        return false;
       }
+      if (tid == 0 && q - 2 >= lo0 && q - 2 + S0 <= hi0) issue(q - 2 + S0);
+      return true;
+    };
+
+    const int qend = z1 - 1 + K;
+    for (int q = lo0; q <= qend; q += 3) {
+      if (!iter(std::integral_constant<int, 0>(), q)) { qf = q; break; }
+      if (q + 1 > qend) break;
+      if (!iter(std::integral_constant<int, 1>(), q + 1)) { qf = q + 1; break; }
+      if (q + 2 > qend) break;
+      if (!iter(std::integral_constant<int, 2>(), q + 2)) { qf = q + 2; break; }
     }
   }
-  return;
+  if (qf < 0) return;
+  // Issued by then: the prologue's planes and plane q'-2+S0 at the end of
+  // every earlier iteration q'.
+  drain_lo = qf + 1;
+  drain_hi = min(hi0, max(lo0 + S0 - 1, qf - 3 + S0));
 
 drain:
   if (tid == 0) {
@@ -198,12 +274,6 @@ drain:
 }
 
 namespace {
-
-template <typename T>
-Coef<T> tb_coef(const void* c) {
-  const T* p = static_cast<const T*>(c);
-  return Coef<T>{p[0], p[1], p[2], p[3], p[4], p[5], p[6]};
-}
 
 template <typename T, int K, int BY, int S0>
 cudaError_t launch_tb_t(const CUtensorMap& src, void* f2, int nx, int ny,
@@ -234,16 +304,15 @@ cudaError_t launch_tb_t(const CUtensorMap& src, void* f2, int nx, int ny,
   const int gz = (nz + zchunk - 1) / zchunk;
   if (info) *info = LaunchInfo{gx, gy, gz, C::THREADS, C::SMEM, zchunk, occ};
   kern<<<dim3(gx, gy, gz), C::THREADS, C::SMEM, stream>>>(
-      src, static_cast<T*>(f2), nx, ny, nz, tb_coef<T>(coef), zchunk, dev_err);
+      src, static_cast<T*>(f2), nx, ny, nz, coef_from<T>(coef), zchunk, dev_err);
   return cudaGetLastError();
 }
 
-// Tile rows and level-0 ring depth per fusion depth (shared memory keeps
-// two CTAs per SM for every K).
+// Tile rows and level-0 ring depth per fusion depth.
 template <int K> struct TbShape;
 template <> struct TbShape<2> { static constexpr int BY = 16, S0 = 5; };
 template <> struct TbShape<3> { static constexpr int BY = 16, S0 = 4; };
-template <> struct TbShape<4> { static constexpr int BY = 8, S0 = 4; };
+template <> struct TbShape<4> { static constexpr int BY = 8, S0 = 5; };
 
 template <typename T>
 cudaError_t launch_tb_dtype(const CUtensorMap& src, void* f2, int nx, int ny,

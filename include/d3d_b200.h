@@ -80,6 +80,14 @@ int d3d_plan_create(int nx, int ny, int nz, int dtype, int kernel,
 #define D3D_NUM_TILE_VARIANTS 5
 int d3d_plan_set_tile(d3d_plan plan, int variant, int zchunk);
 
+/* Enables (default) or disables CUDA-graph replay of d3d_run step loops.
+ * Enabled, the `count` launches of a loop are captured once per (buffers,
+ * count, tile, coefficients) and replayed as one graph launch -- the
+ * replacement for the reference's per-step host launches
+ * (diffusion3d_cuda.cu:361-367).  Loops issued on a stream that is itself
+ * being captured are launched directly into the caller's graph. */
+int d3d_plan_set_graphs(d3d_plan plan, int enable);
+
 int d3d_plan_destroy(d3d_plan plan);
 
 /* JSON description of the plan and its last launch geometry. */
