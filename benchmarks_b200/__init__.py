@@ -26,7 +26,7 @@ D3D_E_INVALID, D3D_E_CUDA, D3D_E_OOM = -1, -2, -3
 D3D_E_TIMEOUT, D3D_E_UNSUPPORTED, D3D_E_BUSY = -4, -5, -6
 F32, F64 = 0, 1
 KERNEL_AUTO, KERNEL_GENERIC, KERNEL_TMA, KERNEL_TB = 0, 1, 2, 3
-NUM_TILE_VARIANTS = 5
+NUM_TILE_VARIANTS = 6
 
 _vp = ctypes.c_void_p
 _vpp = ctypes.POINTER(ctypes.c_void_p)
@@ -42,6 +42,7 @@ _SIGNATURES = {
     "d3d_plan_create": ([_i, _i, _i, _i, _i, _i, _vpp], _i),
     "d3d_plan_set_tile": ([_vp, _i, _i], _i),
     "d3d_plan_set_graphs": ([_vp, _i], _i),
+    "d3d_plan_autotune": ([_vp, _vp, _vp, _vp, _i, _vp, _dp], _i),
     "d3d_plan_destroy": ([_vp], _i),
     "d3d_plan_info": ([_vp, ctypes.c_char_p, _sz], _i),
     "d3d_device_alloc": ([_sz, _vpp], _i),
@@ -166,6 +167,19 @@ class Plan:
 
     def set_tile(self, variant, zchunk=0):
         check(lib().d3d_plan_set_tile(self._h, variant, zchunk))
+
+    def autotune(self, f1, f2, steps=10, coeff=None, stream=None):
+        """Times tile variants / z-chunks on f1, f2 (overwritten); keeps the
+        fastest.  Returns (best ms per step, plan info)."""
+        self._check_buf(f1)
+        self._check_buf(f2)
+        c = self._coeff(coeff)
+        best = ctypes.c_double()
+        check(lib().d3d_plan_autotune(self._h, f1.data_ptr(), f2.data_ptr(),
+                                      c.ctypes.data, steps,
+                                      _stream_handle(stream),
+                                      ctypes.byref(best)))
+        return best.value, self.info()
 
     def set_graphs(self, enable: bool):
         check(lib().d3d_plan_set_graphs(self._h, 1 if enable else 0))

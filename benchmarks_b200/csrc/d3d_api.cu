@@ -358,7 +358,7 @@ int d3d_plan_create(int nx, int ny, int nz, int dtype, int kernel,
   p->dtype = dtype;
   p->kernel = kernel;
   p->tb_depth = kernel == D3D_KERNEL_TB ? tb_depth : 1;
-  p->variant = 0;
+  p->variant = d3d::default_tma_variant(ny);
   p->zchunk = 0;
   p->device = dev;
   p->n = (size_t)nx * ny * nz;
@@ -383,6 +383,56 @@ int d3d_plan_set_tile(d3d_plan p, int variant, int zchunk) {
   p->variant = variant;
   p->zchunk = zchunk;
   for (auto& m : p->maps) m.ptr = nullptr;  // box height may change
+  return D3D_OK;
+}
+
+int d3d_plan_autotune(d3d_plan p, void* f1, void* f2, const void* coeff,
+                      int steps, void* stream, double* best_ms) {
+  if (!p || !f1 || !f2 || !coeff) return fail(D3D_E_INVALID, "NULL argument");
+  if (f1 == f2) return fail(D3D_E_INVALID, "f1 and f2 alias");
+  if (steps < 1) return fail(D3D_E_INVALID, "steps must be >= 1");
+  int rc = check_device(p);
+  if (rc) return rc;
+  cudaStream_t s = as_stream(stream);
+  const bool tb = p->kernel == D3D_KERNEL_TB;
+  if (tb) steps = std::max(steps / p->tb_depth, 1) * p->tb_depth;
+  const int zchunks[] = {0, 16, 32, 64, 128, 256};
+  const int nvariants = tb ? 1 : d3d::kNumTmaVariants;
+  const int old_variant = p->variant, old_zchunk = p->zchunk;
+  float best = -1.0f;
+  int best_v = old_variant, best_z = old_zchunk;
+  for (int v = 0; v < nvariants; ++v) {
+    for (int zc : zchunks) {
+      if (zc != 0 && zc >= p->nz) continue;
+      if (!tb) p->variant = v;
+      p->zchunk = zc;
+      for (auto& m : p->maps) m.ptr = nullptr;
+      void* a = f1;
+      void* b = f2;
+      // one untimed step (attributes, descriptors, caches), then timed
+      rc = run_loop(p, &a, &b, coeff, tb ? p->tb_depth : 1, s);
+      if (rc) break;
+      D3D_TRY(cudaEventRecord(p->ev[0], s), "cudaEventRecord");
+      rc = run_loop(p, &a, &b, coeff, steps, s);
+      if (rc) break;
+      D3D_TRY(cudaEventRecord(p->ev[1], s), "cudaEventRecord");
+      D3D_TRY(cudaEventSynchronize(p->ev[1]), "cudaEventSynchronize");
+      float ms = 0.0f;
+      D3D_TRY(cudaEventElapsedTime(&ms, p->ev[0], p->ev[1]), "elapsed");
+      if (best < 0.0f || ms < best) {
+        best = ms;
+        best_v = p->variant;
+        best_z = zc;
+      }
+    }
+    if (rc) break;
+  }
+  p->variant = rc ? old_variant : best_v;
+  p->zchunk = rc ? old_zchunk : best_z;
+  for (auto& m : p->maps) m.ptr = nullptr;
+  drop_graphs(p);
+  if (rc) return rc;
+  if (best_ms) *best_ms = best / steps;
   return D3D_OK;
 }
 

@@ -17,7 +17,9 @@ struct TmaVariant {
   int by;      // rows of the xy tile
   int stages;  // planes in the shared-memory ring
 };
-constexpr int kNumTmaVariants = 5;
+constexpr int kNumTmaVariants = 6;
+// Default tile variant for a grid with `ny` rows.
+int default_tma_variant(int ny);
 const TmaVariant& tma_variant(int i);
 
 // Launch geometry actually used (for reporting and for the autotuner).

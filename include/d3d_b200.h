@@ -77,7 +77,7 @@ int d3d_plan_create(int nx, int ny, int nz, int dtype, int kernel,
 
 /* Overrides the tile variant (0..D3D_NUM_TILE_VARIANTS-1) and z-chunk
  * (planes per CTA, 0 = automatic) of a plan; used by the autotuner. */
-#define D3D_NUM_TILE_VARIANTS 5
+#define D3D_NUM_TILE_VARIANTS 6
 int d3d_plan_set_tile(d3d_plan plan, int variant, int zchunk);
 
 /* Enables (default) or disables CUDA-graph replay of d3d_run step loops.
@@ -87,6 +87,16 @@ int d3d_plan_set_tile(d3d_plan plan, int variant, int zchunk);
  * (diffusion3d_cuda.cu:361-367).  Loops issued on a stream that is itself
  * being captured are launched directly into the caller's graph. */
 int d3d_plan_set_graphs(d3d_plan plan, int enable);
+
+/* Autotuner (the reference's tile sweep, src/diffusion3d/build.py:9-44,
+ * done at run time instead of by rebuilding): times every tile variant and
+ * a set of z-chunk lengths over `steps` time steps on the caller's buffers
+ * f1/f2 (their contents are overwritten) with CUDA events on `stream`, and
+ * keeps the fastest in the plan.  For D3D_KERNEL_TB plans it tunes the
+ * z-chunk of the fused passes.  *best_ms (may be NULL) receives the best
+ * time per step. */
+int d3d_plan_autotune(d3d_plan plan, void* f1, void* f2, const void* coeff,
+                      int steps, void* stream, double* best_ms);
 
 int d3d_plan_destroy(d3d_plan plan);
 

@@ -238,3 +238,37 @@ def test_device_analytic_close_to_reference_initialize():
     plan32.analytic(o32, float(np.float32(37) * g32[7]))
     ref32 = O.initialize(nx, ny, nz, time=np.float32(37) * g32[7])
     np.testing.assert_allclose(o32.cpu().numpy(), ref32, rtol=1e-5, atol=1e-7)
+
+
+@pytest.mark.parametrize("kernel,tb", [(B.KERNEL_AUTO, 1), (B.KERNEL_TB, 2)])
+def test_autotune_then_bit_exact(kernel, tb):
+    nx, ny, nz = 128, 96, 72
+    c, _ = O.params(nx, ny, nz)
+    plan = B.Plan(nx, ny, nz, B.F32, kernel, tb)
+    s1 = torch.rand((nz, ny, nx), device="cuda")
+    s2 = torch.empty_like(s1)
+    ms, info = plan.autotune(s1, s2, steps=4, coeff=c)
+    assert ms > 0
+    assert 0 <= info["variant"] < B.NUM_TILE_VARIANTS
+    fin = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), 12)
+    f1 = torch.from_numpy(fin).cuda()
+    f2 = torch.empty_like(f1)
+    res, _ = plan.run(f1, f2, 9, c)
+    assert bits_equal(res.cpu().numpy(), O.run(fin, c, 9))
+
+
+def test_graph_replay_matches_direct_launches():
+    nx, ny, nz = 64, 40, 33
+    c, _ = O.params(nx, ny, nz)
+    fin = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), 13)
+    ref = O.run(fin, c, 6)
+    for graphs in (True, False):
+        plan = B.Plan(nx, ny, nz)
+        plan.set_graphs(graphs)
+        f1 = torch.from_numpy(fin).cuda()
+        f2 = torch.empty_like(f1)
+        for _ in range(3):  # replays of the cached graph
+            g1, g2 = f1.clone(), torch.empty_like(f1)
+            res, _ = plan.run(g1, g2, 6, c)
+            assert bits_equal(res.cpu().numpy(), ref)
+        assert plan.info()["graphs"] == int(graphs)
