@@ -57,6 +57,7 @@ _SIGNATURES = {
                       ctypes.POINTER(ctypes.c_float)], _i),
     "d3d_analytic": ([_vp, _vp, ctypes.c_double, _vp], _i),
     "d3d_compare": ([_vp, _vp, _i, _vp, _i, _sz, _dp, _vp], _i),
+    "d3d_compare_noalloc": ([_vp, _i, _vp, _i, _sz, _dp, _vp], _i),
     "d3d_check_device_errors": ([ctypes.POINTER(ctypes.c_uint)], _i),
 }
 
@@ -273,6 +274,23 @@ class Plan:
                                 out.ctypes.data_as(_dp),
                                 _stream_handle(stream)))
         return out
+
+
+NOALLOC_MAX_ELEMENTS = 1 << 28
+
+
+def compare_noalloc(a, b, stream=None):
+    """d3d_compare_noalloc: FP64 (rms, max_abs, max_rel, sum(a)) of device
+    field a against b without any device allocation (n <= 2^28)."""
+    import torch
+    assert a.numel() == b.numel()
+    dt = {torch.float32: F32, torch.float64: F64}
+    out = np.zeros(4, np.float64)
+    check(lib().d3d_compare_noalloc(a.data_ptr(), dt[a.dtype], b.data_ptr(),
+                                    dt[b.dtype], a.numel(),
+                                    out.ctypes.data_as(_dp),
+                                    _stream_handle(stream)))
+    return out
 
 
 def check_device_errors() -> int:

@@ -592,6 +592,32 @@ int d3d_compare(d3d_plan p, const void* a, int a_dtype, const void* b,
   return D3D_OK;
 }
 
+int d3d_compare_noalloc(const void* a, int a_dtype, const void* b,
+                        int b_dtype, size_t n, double out[4], void* stream) {
+  if (!a || !b || !out) return fail(D3D_E_INVALID, "NULL argument");
+  if ((a_dtype != kF32 && a_dtype != kF64) ||
+      (b_dtype != kF32 && b_dtype != kF64))
+    return fail(D3D_E_INVALID, "bad dtype");
+  const size_t max_n = d3d::compare_noalloc_max_elements();
+  if (n > max_n)
+    return fail(D3D_E_INVALID,
+                "n = %zu exceeds the allocation-free limit of %zu elements "
+                "(use d3d_compare for larger fields)",
+                n, max_n);
+  double* scratch = nullptr;
+  D3D_TRY(d3d::noalloc_scratch(&scratch),
+          "cudaGetSymbolAddress (allocation-free scratch)");
+  cudaStream_t s = as_stream(stream);
+  D3D_TRY(d3d::launch_compare_noalloc(a, a_dtype, b, b_dtype, n, scratch, s),
+          "compare launch");
+  g_launches.fetch_add(n ? 2 : 1, std::memory_order_relaxed);
+  D3D_TRY(cudaMemcpyAsync(out, scratch, 4 * sizeof(double),
+                          cudaMemcpyDeviceToHost, s),
+          "D2H copy");
+  D3D_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  return D3D_OK;
+}
+
 int d3d_check_device_errors(unsigned* flags_out) {
   D3D_TRY(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
   unsigned* p = dev_error_ptr();

@@ -68,6 +68,14 @@ cudaError_t launch_compare(const void* a, int a_dtype, const void* b,
                            int b_dtype, size_t n, double* scratch,
                            cudaStream_t stream);
 
+// The allocation-free comparison: same outputs as launch_compare, partial
+// sums in a fixed file-scope device array (n <= compare_noalloc_max_elements).
+size_t compare_noalloc_max_elements();
+cudaError_t noalloc_scratch(double** out);
+cudaError_t launch_compare_noalloc(const void* a, int a_dtype, const void* b,
+                                   int b_dtype, size_t n, double* scratch,
+                                   cudaStream_t stream);
+
 // Analytic solution (the reference's Initialize, computed in FP64 on the
 // device) written in `dtype` at `time`.
 cudaError_t launch_analytic(void* out, int dtype, int nx, int ny, int nz,

@@ -8,6 +8,7 @@
 //   * compare kernels  -- rms, max-abs, max-rel and a checksum accumulated
 //     in double over two device fields of any dtype pair, in a fixed
 //     reduction order (deterministic for a given device).
+#include <atomic>
 #include <cfloat>
 
 #include "d3d_common.cuh"
@@ -132,7 +133,112 @@ cudaError_t launch_partial(const void* a, const void* b, int b_dtype, size_t n,
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free comparison (d3d_compare_noalloc).
+//
+// Some callers cannot allocate device memory when they need the error
+// report: a serving process that has already handed all free HBM to its
+// solve arena, a host whose allocator policy forbids driver allocations
+// behind its back, or code inside a global-mode stream capture, where
+// cudaMalloc is not permitted (and, outside capture, cudaMalloc would
+// synchronise the device in the middle of a latency-sensitive loop).  For
+// them the partial sums live in this fixed file-scope array, which every
+// GPU that loads the library holds until the process exits.
+//
+// Limits and sharing: one partial per kNoAllocChunk elements, at most
+// kNoAllocMaxParts partials, so n <= 2^28 elements (1 GiB of FP32).  Every
+// call uses the same array: a call writes every partial it later reads,
+// so nothing has to start at zero, but two calls whose kernels overlap on
+// the GPU (different streams, no ordering between them) race on it.
+// ---------------------------------------------------------------------------
+constexpr int kNoAllocChunk = 1 << 16;
+constexpr int kNoAllocMaxParts = 1 << 12;
+static __device__ __align__(256) double
+    g_noalloc_scratch[4 * (kNoAllocMaxParts + 1)];  // 128 KiB + 32 B
+
+template <typename TA, typename TB>
+__global__ void __launch_bounds__(kCmpThreads)
+    compare_chunk_kernel(const void* a, const void* b, size_t n,
+                         double* partial) {
+  Acc v = {0, 0, 0, 0};
+  const size_t lo = (size_t)blockIdx.x * kNoAllocChunk;
+  const size_t hi = min(n, lo + kNoAllocChunk);
+  for (size_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const double x = ld_as_double<TA>(a, i);
+    const double y = ld_as_double<TB>(b, i);
+    const double d = x - y;
+    const double ad = fabs(d);
+    v.ss += d * d;
+    v.mx = fmax(v.mx, ad);
+    v.mr = fmax(v.mr, ad / fmax(fabs(y), 1e-300));
+    v.sa += x;
+  }
+  Acc r = block_reduce(v);
+  if (threadIdx.x == 0) {
+    double* p = partial + 4 * (size_t)blockIdx.x;
+    p[0] = r.ss;
+    p[1] = r.mx;
+    p[2] = r.mr;
+    p[3] = r.sa;
+  }
+}
+
+template <typename TA>
+void launch_chunks(const void* a, const void* b, int b_dtype, size_t n,
+                   double* partial, int parts, cudaStream_t s) {
+  if (b_dtype == kF64)
+    compare_chunk_kernel<TA, double>
+        <<<parts, kCmpThreads, 0, s>>>(a, b, n, partial);
+  else
+    compare_chunk_kernel<TA, float>
+        <<<parts, kCmpThreads, 0, s>>>(a, b, n, partial);
+}
+
 }  // namespace
+
+size_t compare_noalloc_max_elements() {
+  return (size_t)kNoAllocMaxParts * kNoAllocChunk;
+}
+
+// Device address of g_noalloc_scratch on the current device.  Looked up
+// once per device (the first allocation-free call on that device) with
+// that device current; in host code the array's name is only a host-side
+// stand-in, never a device address.
+cudaError_t noalloc_scratch(double** out) {
+  static std::atomic<double*> cache[64];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  double* p = cache[dev].load();
+  if (!p) {
+    void* addr = nullptr;
+    e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    p = static_cast<double*>(addr);
+    cache[dev].store(p);
+  }
+  *out = p;
+  return cudaSuccess;
+}
+
+cudaError_t launch_compare_noalloc(const void* a, int a_dtype, const void* b,
+                                   int b_dtype, size_t n, double* scratch,
+                                   cudaStream_t stream) {
+  const int parts = (int)((n + kNoAllocChunk - 1) / kNoAllocChunk);
+  double* partial = scratch + 4;
+  if (parts > 0) {
+    if (a_dtype == kF64)
+      launch_chunks<double>(a, b, b_dtype, n, partial, parts, stream);
+    else
+      launch_chunks<float>(a, b, b_dtype, n, partial, parts, stream);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  compare_final_kernel<<<1, kCmpThreads, 0, stream>>>(partial, parts, n,
+                                                      scratch);
+  return cudaGetLastError();
+}
 
 size_t compare_scratch_bytes() { return (size_t)(kCmpBlocks + 1) * 4 * 8; }
 

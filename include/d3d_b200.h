@@ -149,6 +149,29 @@ int d3d_analytic(d3d_plan plan, void* out, double time, void* stream);
 int d3d_compare(d3d_plan plan, const void* a, int a_dtype, const void* b,
                 int b_dtype, size_t n, double out[4], void* stream);
 
+/* d3d_compare without any device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory at
+ * the moment they want an error report -- a serving loop that has already
+ * given all free HBM to its solve arena, a host whose allocator policy
+ * forbids driver allocations behind its back, or code inside a global-mode
+ * stream capture (where cudaMalloc is not allowed; outside capture it would
+ * also synchronise the device mid-loop).  The caller still passes the two
+ * fields; the partial sums go to a fixed 128 KiB array in the library's
+ * device image, which every GPU that loads the library keeps until exit.
+ *  - n may be at most D3D_NOALLOC_MAX_ELEMENTS (2^28 elements, 1 GiB of
+ *    FP32); larger n returns D3D_E_INVALID without touching the GPU.
+ *  - The first call on a device looks up the array's device address (once
+ *    per device, that device current); make that first call before any
+ *    stream capture.
+ *  - All calls share the array.  Each call writes every slot it reads, so
+ *    results never depend on an earlier call, but calls whose kernels
+ *    overlap on the GPU (different streams with no ordering) race.
+ * Same outputs as d3d_compare (summation order differs: sums agree to
+ * rounding, maxima exactly).  Synchronises `stream`. */
+#define D3D_NOALLOC_MAX_ELEMENTS ((size_t)1 << 28)
+int d3d_compare_noalloc(const void* a, int a_dtype, const void* b,
+                        int b_dtype, size_t n, double out[4], void* stream);
+
 /* Reads and clears the device error word that kernels set instead of
  * trapping when a bounded wait runs out; returns D3D_E_TIMEOUT if any bit
  * was set.  Synchronises the current device. */
