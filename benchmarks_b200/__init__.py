@@ -58,6 +58,14 @@ _SIGNATURES = {
     "d3d_analytic": ([_vp, _vp, ctypes.c_double, _vp], _i),
     "d3d_compare": ([_vp, _vp, _i, _vp, _i, _sz, _dp, _vp], _i),
     "d3d_compare_noalloc": ([_vp, _i, _vp, _i, _sz, _dp, _vp], _i),
+    "d3d_batch_coefficients": ([_i, _i, _i, ctypes.c_float,
+                                ctypes.POINTER(ctypes.c_float)], _i),
+    "d3d_batch_layout": ([_vp, _i, ctypes.POINTER(ctypes.c_size_t)], _i),
+    "d3d_batch_create": ([_vp, _i, _vp, _sz, _vpp], _i),
+    "d3d_batch_autotune": ([_vp, _vp], _i),
+    "d3d_batch_run": ([_vp, _vp, ctypes.POINTER(ctypes.c_float)], _i),
+    "d3d_batch_info": ([_vp, ctypes.c_char_p, _sz], _i),
+    "d3d_batch_destroy": ([_vp], _i),
     "d3d_check_device_errors": ([ctypes.POINTER(ctypes.c_uint)], _i),
 }
 
@@ -274,6 +282,88 @@ class Plan:
                                 out.ctypes.data_as(_dp),
                                 _stream_handle(stream)))
         return out
+
+
+class BatchGrid(ctypes.Structure):
+    """d3d_batch_grid: one grid of a batch."""
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int),
+                ("nz", ctypes.c_int), ("steps", ctypes.c_int),
+                ("coeff", ctypes.c_float * 7),
+                ("offset_a", ctypes.c_ulonglong),
+                ("offset_b", ctypes.c_ulonglong)]
+
+
+def batch_coefficients(nx, ny, nz, kappa):
+    """Stable coefficients for any grid shape (dt from the smallest spacing)."""
+    c = (ctypes.c_float * 7)()
+    check(lib().d3d_batch_coefficients(nx, ny, nz, kappa, c))
+    return np.array(list(c), np.float32)
+
+
+class Batch:
+    """Many independent FP32 grids advanced by the batched multi-grid
+    kernel.  `specs` is a list of (nx, ny, nz, steps, coeff7)."""
+
+    def __init__(self, specs):
+        import torch
+        n = len(specs)
+        arr = (BatchGrid * n)()
+        for i, (nx, ny, nz, steps, coeff) in enumerate(specs):
+            arr[i].nx, arr[i].ny, arr[i].nz, arr[i].steps = nx, ny, nz, steps
+            for j in range(7):
+                arr[i].coeff[j] = float(coeff[j])
+        nbytes = ctypes.c_size_t()
+        check(lib().d3d_batch_layout(arr, n, ctypes.byref(nbytes)))
+        self.grids = arr
+        self.arena = torch.zeros(max(nbytes.value // 4, 1),
+                                 dtype=torch.float32, device="cuda")
+        h = ctypes.c_void_p()
+        check(lib().d3d_batch_create(arr, n, self.arena.data_ptr(),
+                                     nbytes.value, ctypes.byref(h)))
+        self._h = h
+
+    def __len__(self):
+        return len(self.grids)
+
+    def _view(self, i, which):
+        g = self.grids[i]
+        off = g.offset_a if which == 0 else g.offset_b
+        n = g.nx * g.ny * g.nz
+        return self.arena[off:off + n].view(g.nz, g.ny, g.nx)
+
+    def input(self, i):
+        """Device view of grid i's input buffer (write the field here)."""
+        return self._view(i, 0)
+
+    def result(self, i):
+        """Device view of grid i's field after its steps."""
+        return self._view(i, self.grids[i].steps & 1)
+
+    def autotune(self, stream=None):
+        check(lib().d3d_batch_autotune(self._h, _stream_handle(stream)))
+
+    def run(self, stream=None, timed=True):
+        ms = ctypes.c_float()
+        check(lib().d3d_batch_run(self._h, _stream_handle(stream),
+                                  ctypes.byref(ms) if timed else None))
+        return ms.value
+
+    def info(self):
+        import json
+        buf = ctypes.create_string_buffer(4096)
+        check(lib().d3d_batch_info(self._h, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().d3d_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 NOALLOC_MAX_ELEMENTS = 1 << 28

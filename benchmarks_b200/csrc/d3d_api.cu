@@ -101,6 +101,24 @@ void reference_coefficients(int nx, int ny, int nz, T* coeff, T* geom) {
 
 }  // namespace
 
+namespace d3d {
+int set_error(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+int set_cuda_error(cudaError_t e, const char* what) {
+  return cuda_fail(e, what);
+}
+void note_launches(unsigned long long n) {
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+}
+}  // namespace d3d
+
 struct d3d_plan_s {
   int nx, ny, nz, dtype, kernel, tb_depth;
   int variant;  // TMA tile variant

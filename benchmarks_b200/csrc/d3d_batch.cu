@@ -1,0 +1,500 @@
+// Batched solves: many independent FP32 grids advanced together.
+//
+// The reference runs one grid per process (Diffusion3DCUDA::RunKernel,
+// diffusion3d_cuda.cu:353-371).  Here a batch of grids of different shapes,
+// coefficients and step counts is advanced by one multi-grid step kernel
+// per time step; all steps of a run are captured once into a CUDA graph and
+// replayed as a single graph launch.
+//
+// Work list.  Grids are split into size classes by nx; each class has one
+// tile shape (BX x BY, 256 threads), picked by the autotuner.  Within a
+// class, grids are sorted by step count (descending) and every grid
+// contributes one work item per xy tile, so the items still active at step
+// s are a prefix of the class's list: step s launches exactly that prefix.
+//
+// Tile kernel (march_tile).  A CTA marches its tile through all nz planes.
+// Each thread owns its interior cell and at most one halo cell, and keeps
+// the next P planes of both in a register queue (loads in flight), stores
+// the current plane into one of two shared halo planes (one __syncthreads
+// per plane), takes n/s/w/e from shared memory and b/c/t from its queue.
+// Every load address is clamped into the grid, which is exactly the
+// reference's replicated-neighbour boundary, so no value is ever selected.
+// Each point is d3d::point: results are bit-identical to running each grid
+// alone.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "d3d_b200.h"
+#include "d3d_common.cuh"
+#include "d3d_kernels.h"
+
+namespace d3d {
+
+struct BatchDesc {
+  float* a;
+  float* b;
+  int nx, ny, nz, tiles_x;
+  Coef<float> k;
+};
+
+template <int BX, int BY>
+struct BTile {
+  static constexpr int THREADS = BX * BY;
+  static constexpr int W = BX + 2;
+  static constexpr int H = BY + 2;
+  static constexpr int E = W * H;
+  static constexpr int HALO = E - BX * BY;
+  static_assert(THREADS == 256, "tile kernels run 256 threads");
+  static_assert(HALO <= THREADS, "one halo cell per thread at most");
+};
+
+constexpr int kQ = 4;  // planes in each thread's register queue
+
+// One plane's loads for this thread: its interior cell and its halo cell.
+struct Pair {
+  float own, halo;
+};
+
+template <int BX, int BY>
+__device__ __forceinline__ void march_tile(const float* __restrict__ src,
+                                           float* __restrict__ dst, int nx,
+                                           int ny, int nz, int x0, int y0,
+                                           const Coef<float>& k,
+                                           float (*stage)[BTile<BX, BY>::E]) {
+  using TL = BTile<BX, BY>;
+  const int tid = threadIdx.x;
+  const int tx = tid % BX, ty = tid / BX;
+  const int xg = x0 + tx, yg = y0 + ty;
+  // Interior cell: stage index and clamped in-plane offset.
+  const int own_s = (ty + 1) * TL::W + (tx + 1);
+  const int own_g = min(yg, ny - 1) * nx + min(xg, nx - 1);
+  // Halo cell h = tid (if any): the border of the W x H box.
+  const bool has_halo = tid < TL::HALO;
+  int lx = 0, ly = 0;
+  {
+    const int h = tid;
+    if (h < TL::W) {
+      lx = h;
+      ly = 0;
+    } else if (h < 2 * TL::W) {
+      lx = h - TL::W;
+      ly = TL::H - 1;
+    } else if (h < 2 * TL::W + TL::H - 2) {
+      lx = 0;
+      ly = 1 + h - 2 * TL::W;
+    } else {
+      lx = TL::W - 1;
+      ly = 1 + h - 2 * TL::W - (TL::H - 2);
+    }
+  }
+  const int halo_s = ly * TL::W + lx;
+  const int hx = min(max(x0 - 1 + lx, 0), nx - 1);
+  const int hy = min(max(y0 - 1 + ly, 0), ny - 1);
+  const int halo_g = hy * nx + hx;
+  const bool store_ok = xg < nx && yg < ny;
+  const size_t plane = (size_t)nx * ny;
+
+  auto load = [&](int p) -> Pair {
+    const float* pl = src + (size_t)min(p, nz - 1) * plane;
+    Pair v;
+    v.own = __ldg(pl + own_g);
+    v.halo = has_halo ? __ldg(pl + halo_g) : 0.0f;
+    return v;
+  };
+
+  Pair q0 = load(0), q1 = load(1), q2 = load(2), q3 = load(3);
+  float b = q0.own;  // plane -1 is plane 0
+
+  // One plane: publish `cur`, refill its slot with plane z+kQ, compute.
+  auto plane_step = [&](int z, Pair& cur, const Pair& next) {
+    float* st = stage[z & 1];
+    st[own_s] = cur.own;
+    if (has_halo) st[halo_s] = cur.halo;
+    const float c = cur.own;
+    const float t = next.own;  // plane min(z+1, nz-1)
+    cur = load(z + kQ);
+    __syncthreads();
+    const float w = st[own_s - 1];
+    const float e = st[own_s + 1];
+    const float n = st[own_s - TL::W];
+    const float s = st[own_s + TL::W];
+    const float v = point(k, c, w, e, s, n, b, t);
+    if (store_ok) dst[(size_t)z * plane + (size_t)yg * nx + xg] = v;
+    b = c;
+  };
+
+  for (int z = 0; z < nz; z += kQ) {
+    plane_step(z, q0, q1);
+    if (z + 1 >= nz) break;
+    plane_step(z + 1, q1, q2);
+    if (z + 2 >= nz) break;
+    plane_step(z + 2, q2, q3);
+    if (z + 3 >= nz) break;
+    plane_step(z + 3, q3, q0);
+  }
+}
+
+template <int BX, int BY>
+__global__ void __launch_bounds__(256)
+    batch_step_kernel(const BatchDesc* __restrict__ descs,
+                      const int2* __restrict__ items, int parity) {
+  __shared__ float stage[2][BTile<BX, BY>::E];
+  const int2 it = items[blockIdx.x];
+  const BatchDesc d = descs[it.x];
+  const int bx = it.y % d.tiles_x, by = it.y / d.tiles_x;
+  const float* src = parity ? d.b : d.a;
+  float* dst = parity ? d.a : d.b;
+  march_tile<BX, BY>(src, dst, d.nx, d.ny, d.nz, bx * BX, by * BY, d.k,
+                     stage);
+}
+
+// Tile shapes the batch kernel is instantiated for.
+struct BShape {
+  int bx, by;
+};
+constexpr int kNumBShapes = 3;
+const BShape kBShapes[kNumBShapes] = {{32, 8}, {16, 16}, {64, 4}};
+
+cudaError_t launch_batch_step(int shape, const BatchDesc* descs,
+                              const int2* items, int nitems, int parity,
+                              cudaStream_t s) {
+  if (nitems <= 0) return cudaSuccess;
+  switch (shape) {
+    case 0: batch_step_kernel<32, 8><<<nitems, 256, 0, s>>>(descs, items, parity); break;
+    case 1: batch_step_kernel<16, 16><<<nitems, 256, 0, s>>>(descs, items, parity); break;
+    case 2: batch_step_kernel<64, 4><<<nitems, 256, 0, s>>>(descs, items, parity); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace d3d
+
+// ---------------------------------------------------------------------------
+// Host side of the batch API (C ABI in include/d3d_b200.h)
+// ---------------------------------------------------------------------------
+namespace {
+
+using d3d::BatchDesc;
+using d3d::kBShapes;
+using d3d::kNumBShapes;
+
+// Size classes by nx; the autotuner picks one tile shape per class.
+constexpr int kNumClasses = 4;
+int class_of(int nx) {
+  if (nx <= 24) return 0;
+  if (nx <= 40) return 1;
+  if (nx <= 72) return 2;
+  return 3;
+}
+
+struct ClassPlan {
+  std::vector<int> grids;  // batch indices, sorted by steps descending
+  int shape = 0;
+  int max_steps = 0;
+  std::vector<int> active;  // items active at step s
+  BatchDesc* d_descs = nullptr;
+  int2* d_items = nullptr;
+  int nitems = 0;
+};
+
+}  // namespace
+
+struct d3d_batch_s {
+  std::vector<d3d_batch_grid> grids;
+  float* arena = nullptr;
+  size_t arena_bytes = 0;
+  int max_steps = 0;
+  ClassPlan cls[kNumClasses];
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t capture_stream = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  int device = 0;
+  long long total_items = 0;
+  unsigned long long launches_per_run = 0;
+};
+
+namespace {
+
+int bfail(int code, const char* msg) { return d3d::set_error(code, "%s", msg); }
+
+int bcuda(cudaError_t e, const char* what) {
+  return d3d::set_cuda_error(e, what);
+}
+
+#define B_TRY(call, what)                            \
+  do {                                               \
+    cudaError_t e__ = (call);                        \
+    if (e__ != cudaSuccess) return bcuda(e__, what); \
+  } while (0)
+
+// (Re)builds one class's descriptors and item list for its current shape.
+int build_class(d3d_batch b, ClassPlan& c) {
+  if (c.d_descs) cudaFree(c.d_descs);
+  if (c.d_items) cudaFree(c.d_items);
+  c.d_descs = nullptr;
+  c.d_items = nullptr;
+  c.active.assign(c.max_steps, 0);
+  c.nitems = 0;
+  if (c.grids.empty()) return D3D_OK;
+  const d3d::BShape sh = kBShapes[c.shape];
+  std::vector<BatchDesc> descs;
+  std::vector<int2> items;
+  for (size_t gi = 0; gi < c.grids.size(); ++gi) {
+    const d3d_batch_grid& g = b->grids[c.grids[gi]];
+    BatchDesc d;
+    d.a = b->arena + g.offset_a;
+    d.b = b->arena + g.offset_b;
+    d.nx = g.nx;
+    d.ny = g.ny;
+    d.nz = g.nz;
+    d.tiles_x = (g.nx + sh.bx - 1) / sh.bx;
+    const int tiles = d.tiles_x * ((g.ny + sh.by - 1) / sh.by);
+    d.k = d3d::Coef<float>{g.coeff[0], g.coeff[1], g.coeff[2], g.coeff[3],
+                           g.coeff[4], g.coeff[5], g.coeff[6], -0.0f};
+    descs.push_back(d);
+    for (int t = 0; t < tiles; ++t) items.push_back(make_int2((int)gi, t));
+    // items of this grid are active for steps [0, g.steps)
+    for (int s = 0; s < g.steps; ++s) c.active[s] += tiles;
+  }
+  c.nitems = (int)items.size();
+  B_TRY(cudaMalloc(&c.d_descs, descs.size() * sizeof(BatchDesc)),
+        "cudaMalloc (batch descriptors)");
+  B_TRY(cudaMalloc(&c.d_items, items.size() * sizeof(int2)),
+        "cudaMalloc (batch items)");
+  B_TRY(cudaMemcpy(c.d_descs, descs.data(), descs.size() * sizeof(BatchDesc),
+                   cudaMemcpyHostToDevice),
+        "H2D descriptors");
+  B_TRY(cudaMemcpy(c.d_items, items.data(), items.size() * sizeof(int2),
+                   cudaMemcpyHostToDevice),
+        "H2D items");
+  return D3D_OK;
+}
+
+// All steps of all classes, in step order (class launches of one step are
+// independent; steps depend on each other through the stream order).
+int enqueue_run(d3d_batch b, cudaStream_t s, int only_class, int max_steps,
+                unsigned long long* launches) {
+  unsigned long long n = 0;
+  for (int step = 0; step < max_steps; ++step) {
+    for (int ci = 0; ci < kNumClasses; ++ci) {
+      if (only_class >= 0 && ci != only_class) continue;
+      ClassPlan& c = b->cls[ci];
+      if (step >= c.max_steps || c.active[step] == 0) continue;
+      B_TRY(d3d::launch_batch_step(c.shape, c.d_descs, c.d_items,
+                                   c.active[step], step & 1, s),
+            "batch step launch");
+      ++n;
+    }
+  }
+  if (launches) *launches = n;
+  return D3D_OK;
+}
+
+void drop_graph(d3d_batch b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  b->exec = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int d3d_batch_coefficients(int nx, int ny, int nz, float kappa,
+                           float coeff7[7]) {
+  if (nx < 1 || ny < 1 || nz < 1 || !(kappa > 0.0f) || !coeff7)
+    return bfail(D3D_E_INVALID, "bad grid or kappa");
+  const float l = 1.0f;
+  const float dx = l / nx, dy = l / ny, dz = l / nz;
+  const float h = std::min(dx, std::min(dy, dz));
+  const float dt = (float)(0.1 * h * h / kappa);
+  const float ce = kappa * dt / (dx * dx);
+  const float cn = kappa * dt / (dy * dy);
+  const float ct = kappa * dt / (dz * dz);
+  const float cc = (float)(1.0 - (ce + ce + cn + cn + ct + ct));
+  const float c[7] = {ce, ce, cn, cn, ct, ct, cc};
+  memcpy(coeff7, c, sizeof c);
+  return D3D_OK;
+}
+
+int d3d_batch_layout(d3d_batch_grid* grids, int n, size_t* arena_bytes) {
+  if (!grids || n < 0 || !arena_bytes) return bfail(D3D_E_INVALID, "NULL");
+  unsigned long long off = 0;  // elements
+  for (int i = 0; i < n; ++i) {
+    const unsigned long long pts =
+        (unsigned long long)grids[i].nx * grids[i].ny * grids[i].nz;
+    const unsigned long long padded = (pts + 63) / 64 * 64;  // 256 B
+    grids[i].offset_a = off;
+    grids[i].offset_b = off + padded;
+    off += 2 * padded;
+  }
+  *arena_bytes = (size_t)off * sizeof(float);
+  return D3D_OK;
+}
+
+int d3d_batch_create(const d3d_batch_grid* grids, int n, void* arena,
+                     size_t arena_bytes, d3d_batch* out) {
+  if (!grids || n < 1 || !arena || !out)
+    return bfail(D3D_E_INVALID, "NULL argument or empty batch");
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    const d3d_batch_grid& g = grids[i];
+    if (g.nx < 1 || g.ny < 1 || g.nz < 1 || g.steps < 0)
+      return bfail(D3D_E_INVALID, "bad grid dimensions or steps");
+    if ((long long)g.nx * g.ny >= (1LL << 31))
+      return bfail(D3D_E_INVALID, "grid plane too large");
+    const unsigned long long pts = (unsigned long long)g.nx * g.ny * g.nz;
+    if ((g.offset_a + pts) * 4 > arena_bytes ||
+        (g.offset_b + pts) * 4 > arena_bytes)
+      return bfail(D3D_E_INVALID, "grid buffer outside the arena");
+    const unsigned long long a0 = g.offset_a, a1 = g.offset_a + pts;
+    const unsigned long long b0 = g.offset_b, b1 = g.offset_b + pts;
+    if (a0 < b1 && b0 < a1)
+      return bfail(D3D_E_INVALID, "a grid's two buffers overlap");
+  }
+  d3d_batch b = new (std::nothrow) d3d_batch_s();
+  if (!b) return bfail(D3D_E_OOM, "batch allocation");
+  b->grids.assign(grids, grids + n);
+  b->arena = static_cast<float*>(arena);
+  b->arena_bytes = arena_bytes;
+  cudaGetDevice(&b->device);
+  for (int i = 0; i < n; ++i) {
+    ClassPlan& c = b->cls[class_of(grids[i].nx)];
+    c.grids.push_back(i);
+    c.max_steps = std::max(c.max_steps, grids[i].steps);
+    b->max_steps = std::max(b->max_steps, grids[i].steps);
+  }
+  for (auto& c : b->cls) {
+    std::stable_sort(c.grids.begin(), c.grids.end(), [&](int x, int y) {
+      return b->grids[x].steps > b->grids[y].steps;
+    });
+    c.shape = 0;
+    int rc = build_class(b, c);
+    if (rc) {
+      d3d_batch_destroy(b);
+      return rc;
+    }
+    for (int s = 0; s < c.max_steps; ++s) b->total_items += c.active[s];
+  }
+  if (cudaEventCreate(&b->ev[0]) != cudaSuccess ||
+      cudaEventCreate(&b->ev[1]) != cudaSuccess) {
+    d3d_batch_destroy(b);
+    return bfail(D3D_E_CUDA, "cudaEventCreate");
+  }
+  *out = b;
+  return D3D_OK;
+}
+
+int d3d_batch_autotune(d3d_batch b, void* stream) {
+  if (!b) return bfail(D3D_E_INVALID, "NULL batch");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  drop_graph(b);
+  for (int ci = 0; ci < kNumClasses; ++ci) {
+    ClassPlan& c = b->cls[ci];
+    if (c.grids.empty()) continue;
+    const int probe_steps = std::min(c.max_steps, 8);
+    if (probe_steps == 0) continue;
+    float best = -1.0f;
+    int best_shape = c.shape;
+    for (int sh = 0; sh < kNumBShapes; ++sh) {
+      c.shape = sh;
+      int rc = build_class(b, c);
+      if (rc) return rc;
+      rc = enqueue_run(b, s, ci, 1, nullptr);  // warm-up
+      if (rc) return rc;
+      B_TRY(cudaEventRecord(b->ev[0], s), "cudaEventRecord");
+      rc = enqueue_run(b, s, ci, probe_steps, nullptr);
+      if (rc) return rc;
+      B_TRY(cudaEventRecord(b->ev[1], s), "cudaEventRecord");
+      B_TRY(cudaEventSynchronize(b->ev[1]), "cudaEventSynchronize");
+      float ms = 0.0f;
+      B_TRY(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]), "elapsed");
+      if (best < 0.0f || ms < best) {
+        best = ms;
+        best_shape = sh;
+      }
+    }
+    c.shape = best_shape;
+    int rc = build_class(b, c);
+    if (rc) return rc;
+  }
+  return D3D_OK;
+}
+
+int d3d_batch_run(d3d_batch b, void* stream, float* kernel_ms) {
+  if (!b) return bfail(D3D_E_INVALID, "NULL batch");
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (dev != b->device) return bfail(D3D_E_INVALID, "wrong device");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (!b->exec) {
+    if (!b->capture_stream)
+      B_TRY(cudaStreamCreateWithFlags(&b->capture_stream,
+                                      cudaStreamNonBlocking),
+            "cudaStreamCreateWithFlags");
+    B_TRY(cudaStreamBeginCapture(b->capture_stream,
+                                 cudaStreamCaptureModeThreadLocal),
+          "cudaStreamBeginCapture");
+    int rc = enqueue_run(b, b->capture_stream, -1, b->max_steps,
+                         &b->launches_per_run);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->capture_stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return bcuda(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&b->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      b->exec = nullptr;
+      return bcuda(e, "cudaGraphInstantiate");
+    }
+  }
+  B_TRY(cudaEventRecord(b->ev[0], s), "cudaEventRecord");
+  B_TRY(cudaGraphLaunch(b->exec, s), "cudaGraphLaunch");
+  B_TRY(cudaEventRecord(b->ev[1], s), "cudaEventRecord");
+  d3d::note_launches(b->launches_per_run);
+  if (kernel_ms) {
+    B_TRY(cudaEventSynchronize(b->ev[1]), "cudaEventSynchronize");
+    B_TRY(cudaEventElapsedTime(kernel_ms, b->ev[0], b->ev[1]), "elapsed");
+  }
+  return D3D_OK;
+}
+
+int d3d_batch_info(d3d_batch b, char* buf, size_t len) {
+  if (!b || !buf) return bfail(D3D_E_INVALID, "NULL argument");
+  int used = snprintf(buf, len,
+                      "{\"grids\": %zu, \"max_steps\": %d, \"items\": %lld, "
+                      "\"launches_per_run\": %llu, \"classes\": [",
+                      b->grids.size(), b->max_steps, b->total_items,
+                      b->launches_per_run);
+  for (int ci = 0; ci < kNumClasses && used < (int)len; ++ci) {
+    const ClassPlan& c = b->cls[ci];
+    used += snprintf(buf + used, len - used,
+                     "%s{\"grids\": %zu, \"tile\": [%d, %d], \"items\": %d}",
+                     ci ? ", " : "", c.grids.size(), kBShapes[c.shape].bx,
+                     kBShapes[c.shape].by, c.nitems);
+  }
+  if (used < (int)len) snprintf(buf + used, len - used, "]}");
+  return D3D_OK;
+}
+
+int d3d_batch_destroy(d3d_batch b) {
+  if (!b) return D3D_OK;
+  drop_graph(b);
+  for (auto& c : b->cls) {
+    if (c.d_descs) cudaFree(c.d_descs);
+    if (c.d_items) cudaFree(c.d_items);
+  }
+  if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
+  if (b->ev[0]) cudaEventDestroy(b->ev[0]);
+  if (b->ev[1]) cudaEventDestroy(b->ev[1]);
+  delete b;
+  return D3D_OK;
+}
+
+}  // extern "C"

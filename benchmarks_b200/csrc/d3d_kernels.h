@@ -8,6 +8,13 @@
 
 namespace d3d {
 
+// Error and launch bookkeeping shared by every C-ABI translation unit
+// (defined in d3d_api.cu): the calling thread's last-error text and the
+// process-wide count of kernel launches.
+int set_error(int code, const char* fmt, ...);
+int set_cuda_error(cudaError_t e, const char* what);
+void note_launches(unsigned long long n);
+
 enum Dtype { kF32 = 0, kF64 = 1 };
 
 inline size_t dtype_size(int dtype) { return dtype == kF64 ? 8 : 4; }

@@ -149,6 +149,61 @@ int d3d_analytic(d3d_plan plan, void* out, double time, void* stream);
 int d3d_compare(d3d_plan plan, const void* a, int a_dtype, const void* b,
                 int b_dtype, size_t n, double out[4], void* stream);
 
+/* ---------------------------------------------------------------------
+ * Batched solves: many independent FP32 grids of different shapes,
+ * coefficients and step counts advanced by ONE persistent multi-grid
+ * kernel.  No counterpart in the reference (which runs one grid per
+ * process); each grid's arithmetic is still RunKernel's, so every grid's
+ * result is bit-identical to running it alone (with the reference or with
+ * d3d_run).
+ *
+ * Fields live in one caller-owned device arena.  Grid i uses two buffers
+ * of nx*ny*nz floats at element offsets offset_a and offset_b; its input
+ * is in buffer a, and after the run its result is in buffer a when steps
+ * is even and in buffer b when steps is odd (the reference's ping-pong).
+ * --------------------------------------------------------------------- */
+typedef struct {
+  int nx, ny, nz, steps;
+  float coeff[7];              /* ce, cw, cn, cs, ct, cb, cc */
+  unsigned long long offset_a; /* element offsets into the arena */
+  unsigned long long offset_b;
+} d3d_batch_grid;
+
+typedef struct d3d_batch_s* d3d_batch;
+
+/* Coefficients for a grid of any shape: like the reference constructor
+ * (diffusion3d.h:54-66) but with dt = 0.1*h^2/kappa for h = min(dx, dy, dz),
+ * which keeps cc >= 0.4 (the reference derives dt from dx alone, which
+ * makes non-cubic grids with ny or nz > nx unstable). */
+int d3d_batch_coefficients(int nx, int ny, int nz, float kappa,
+                           float coeff7[7]);
+
+/* Packs grids back to back (two buffers each, 256-byte aligned) and sets
+ * their offsets; *arena_bytes receives the arena size needed. */
+int d3d_batch_layout(d3d_batch_grid* grids, int n, size_t* arena_bytes);
+
+/* Builds the batch: descriptors, size classes, and the work queue (grids
+ * ordered by step count and packed into waves whose fields fit in L2).
+ * `arena` must stay valid for the batch's lifetime. */
+int d3d_batch_create(const d3d_batch_grid* grids, int n, void* arena,
+                     size_t arena_bytes, d3d_batch* out);
+
+/* Times each tile shape per size class on the batch's own grids (their
+ * fields are overwritten) and keeps the fastest per class. */
+int d3d_batch_autotune(d3d_batch batch, void* stream);
+
+/* Runs every grid for its step count: one cooperative persistent launch
+ * (replayed from a CUDA graph after the first run).  *kernel_ms (may be
+ * NULL) receives the device time.  Returns D3D_E_TIMEOUT if a bounded
+ * inter-CTA wait ran out (the kernel then exits early; results are
+ * invalid). */
+int d3d_batch_run(d3d_batch batch, void* stream, float* kernel_ms);
+
+/* JSON summary: grids, waves, work items, tile shape per class, CTAs. */
+int d3d_batch_info(d3d_batch batch, char* buf, size_t len);
+
+int d3d_batch_destroy(d3d_batch batch);
+
 /* d3d_compare without any device allocation.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory at
  * the moment they want an error report -- a serving loop that has already

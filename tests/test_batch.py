@@ -1,0 +1,163 @@
+"""Batched solves (d3d_batch_*): many grids of different shapes, coefficients
+and step counts in one run.  Every grid's result must be bit-identical to
+the oracle's RunKernel on that grid, and to the same grid run alone."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import benchmarks_b200 as B
+import oracle as O
+
+
+def policy_coefficients(nx, ny, nz, kappa):
+    """The stability policy in plain float32 arithmetic: the reference's
+    constructor expressions with dt from the smallest spacing."""
+    f = np.float32
+    dx, dy, dz = f(1.0) / f(nx), f(1.0) / f(ny), f(1.0) / f(nz)
+    h = min(dx, dy, dz)
+    dt = f(0.1 * float(h) * float(h) / float(f(kappa)))
+    k = f(kappa)
+    ce = k * dt / (dx * dx)
+    cn = k * dt / (dy * dy)
+    ct = k * dt / (dz * dz)
+    cc = f(1.0 - float(ce + ce + cn + cn + ct + ct))
+    return np.array([ce, ce, cn, cn, ct, ct, cc], np.float32)
+
+
+@pytest.mark.parametrize("dims,kappa", [((16, 96, 40), 0.1),
+                                        ((96, 16, 17), 0.05),
+                                        ((33, 33, 33), 0.2),
+                                        ((64, 64, 64), 0.1)])
+def test_policy_coefficients(dims, kappa):
+    c = B.batch_coefficients(*dims, kappa)
+    assert c.tobytes() == policy_coefficients(*dims, kappa).tobytes()
+    assert c[6] >= 0.39  # stable: cc >= 0.4 up to rounding
+    if dims[0] == dims[1] == dims[2] and kappa == np.float32(0.1):
+        # cubic grids: the reference constructor's coefficients
+        assert c.tobytes() == O.params(*dims)[0].tobytes()
+
+
+def test_layout_packs_aligned_disjoint_buffers():
+    specs = [(17, 5, 3, 1), (96, 80, 33, 4), (16, 16, 16, 0)]
+    arr = (B.BatchGrid * len(specs))()
+    for i, (nx, ny, nz, st) in enumerate(specs):
+        arr[i].nx, arr[i].ny, arr[i].nz, arr[i].steps = nx, ny, nz, st
+    nbytes = ctypes.c_size_t()
+    B.check(B.lib().d3d_batch_layout(arr, len(specs), ctypes.byref(nbytes)))
+    spans = []
+    for g in arr:
+        n = g.nx * g.ny * g.nz
+        for off in (g.offset_a, g.offset_b):
+            assert (off * 4) % 256 == 0
+            spans.append((off, off + n))
+    spans.sort()
+    for (a0, a1), (b0, b1) in zip(spans, spans[1:]):
+        assert a1 <= b0
+    assert spans[-1][1] * 4 <= nbytes.value
+
+
+def test_create_rejects_bad_batches():
+    L = B.lib()
+    arr = (B.BatchGrid * 1)()
+    arr[0].nx, arr[0].ny, arr[0].nz, arr[0].steps = 8, 8, 8, 1
+    arr[0].offset_a, arr[0].offset_b = 0, 256
+    h = ctypes.c_void_p()
+    # second buffer past the end of the arena
+    assert L.d3d_batch_create(arr, 1, 4096, 1024 * 4,
+                              ctypes.byref(h)) == B.D3D_E_INVALID
+    # overlapping buffers
+    arr[0].offset_b = 100
+    assert L.d3d_batch_create(arr, 1, 4096, 4096 * 4,
+                              ctypes.byref(h)) == B.D3D_E_INVALID
+    arr[0].nx = 0
+    assert L.d3d_batch_create(arr, 1, 4096, 4096 * 4,
+                              ctypes.byref(h)) == B.D3D_E_INVALID
+
+
+def _mixed_specs(seed, n, max_side=40, max_steps=24):
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(n):
+        nx, ny, nz = (int(v) for v in rng.integers(1, max_side + 1, 3))
+        steps = int(rng.integers(0, max_steps + 1))
+        kappa = float(rng.uniform(0.05, 0.2))
+        specs.append((nx, ny, nz, steps, B.batch_coefficients(nx, ny, nz,
+                                                              kappa)))
+    return specs
+
+
+def _fields(specs, seed):
+    out = []
+    for i, (nx, ny, nz, _, _) in enumerate(specs):
+        f = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), seed + i)
+        out.append(f)
+    return out
+
+
+def _run_batch(specs, fields, autotune=False):
+    torch = pytest.importorskip("torch")
+    batch = B.Batch(specs)
+    if autotune:
+        batch.autotune()
+    for i, f in enumerate(fields):
+        batch.input(i).copy_(torch.from_numpy(f))
+    batch.run()
+    torch.cuda.synchronize()
+    return [batch.result(i).cpu().numpy() for i in range(len(specs))], batch
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [1, 2])
+def test_batch_bit_exact_vs_oracle(seed):
+    specs = _mixed_specs(seed, 40)
+    # include the edge shapes explicitly
+    specs += [(1, 1, 1, 5, B.batch_coefficients(1, 1, 1, 0.1)),
+              (96, 3, 2, 7, B.batch_coefficients(96, 3, 2, 0.1)),
+              (70, 70, 9, 11, B.batch_coefficients(70, 70, 9, 0.15)),
+              (20, 20, 20, 0, B.batch_coefficients(20, 20, 20, 0.1))]
+    fields = _fields(specs, 100 * seed)
+    outs, batch = _run_batch(specs, fields)
+    for (nx, ny, nz, steps, c), f, o in zip(specs, fields, outs):
+        ref = O.run(f, c, steps)
+        assert o.tobytes() == ref.tobytes(), (nx, ny, nz, steps)
+    info = batch.info()
+    assert info["grids"] == len(specs)
+
+
+@pytest.mark.gpu
+def test_each_grid_same_alone_and_in_the_mix():
+    specs = _mixed_specs(7, 24, max_side=64, max_steps=16)
+    fields = _fields(specs, 700)
+    mixed, _ = _run_batch(specs, fields)
+    for i in (0, 5, 11, 23):
+        alone, _ = _run_batch([specs[i]], [fields[i]])
+        assert alone[0].tobytes() == mixed[i].tobytes()
+
+
+@pytest.mark.gpu
+def test_autotuned_batch_still_bit_exact():
+    specs = _mixed_specs(3, 30, max_side=96, max_steps=10)
+    fields = _fields(specs, 300)
+    outs, batch = _run_batch(specs, fields, autotune=True)
+    for (nx, ny, nz, steps, c), f, o in zip(specs, fields, outs):
+        assert o.tobytes() == O.run(f, c, steps).tobytes()
+    shapes = {tuple(c["tile"]) for c in batch.info()["classes"]}
+    assert shapes <= {(32, 8), (16, 16), (64, 4)}
+
+
+@pytest.mark.gpu
+def test_batch_replay_is_repeatable():
+    torch = pytest.importorskip("torch")
+    specs = _mixed_specs(9, 12, max_side=48, max_steps=9)
+    fields = _fields(specs, 900)
+    batch = B.Batch(specs)
+    results = []
+    for _ in range(3):  # the graph is captured once and replayed
+        for i, f in enumerate(fields):
+            batch.input(i).copy_(torch.from_numpy(f))
+        batch.run()
+        torch.cuda.synchronize()
+        results.append([batch.result(i).cpu().numpy().tobytes()
+                        for i in range(len(specs))])
+    assert results[0] == results[1] == results[2]
