@@ -66,6 +66,17 @@ _SIGNATURES = {
     "d3d_batch_run": ([_vp, _vp, ctypes.POINTER(ctypes.c_float)], _i),
     "d3d_batch_info": ([_vp, ctypes.c_char_p, _sz], _i),
     "d3d_batch_destroy": ([_vp], _i),
+    "d3d_server_create": ([_sz, _i, _vpp], _i),
+    "d3d_server_submit": ([_vp, _i, _i, _i, _i,
+                           ctypes.POINTER(ctypes.c_float), _vp, _vp,
+                           ctypes.POINTER(ctypes.c_longlong)], _i),
+    "d3d_server_tick": ([_vp, ctypes.POINTER(ctypes.c_longlong), _i,
+                         ctypes.POINTER(ctypes.c_int)], _i),
+    "d3d_server_pending": ([_vp, ctypes.POINTER(ctypes.c_int),
+                            ctypes.POINTER(ctypes.c_int),
+                            ctypes.POINTER(ctypes.c_int)], _i),
+    "d3d_server_stats": ([_vp, ctypes.c_char_p, _sz], _i),
+    "d3d_server_destroy": ([_vp], _i),
     "d3d_check_device_errors": ([ctypes.POINTER(ctypes.c_uint)], _i),
 }
 
@@ -357,6 +368,74 @@ class Batch:
     def close(self):
         if getattr(self, "_h", None):
             lib().d3d_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching solve server (d3d_server_*).  submit() queues a
+    solve with host input/output arrays (C-contiguous float32; pinned for
+    asynchronous copies); tick() runs one scheduling round and returns the
+    ids that finished."""
+
+    def __init__(self, arena_bytes, chunk=8):
+        h = ctypes.c_void_p()
+        check(lib().d3d_server_create(int(arena_bytes), chunk,
+                                      ctypes.byref(h)))
+        self._h = h
+        self._keep = {}
+        self._ids = (ctypes.c_longlong * 4096)()
+
+    def submit(self, host_in, host_out, steps, coeff):
+        assert host_in.dtype == np.float32 and host_out.dtype == np.float32
+        assert host_in.flags["C_CONTIGUOUS"] and host_out.flags["C_CONTIGUOUS"]
+        assert host_in.shape == host_out.shape and host_in.ndim == 3
+        nz, ny, nx = host_in.shape
+        c = (ctypes.c_float * 7)(*[float(v) for v in coeff])
+        rid = ctypes.c_longlong()
+        check(lib().d3d_server_submit(self._h, nx, ny, nz, steps, c,
+                                      host_in.ctypes.data,
+                                      host_out.ctypes.data,
+                                      ctypes.byref(rid)))
+        self._keep[rid.value] = (host_in, host_out)
+        return rid.value
+
+    def tick(self):
+        n = ctypes.c_int()
+        check(lib().d3d_server_tick(self._h, self._ids, len(self._ids),
+                                    ctypes.byref(n)))
+        done = [self._ids[i] for i in range(n.value)]
+        for i in done:
+            self._keep.pop(i, None)
+        return done
+
+    def pending(self):
+        q, a, r = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().d3d_server_pending(self._h, ctypes.byref(q),
+                                       ctypes.byref(a), ctypes.byref(r)))
+        return q.value, a.value, r.value
+
+    def drain(self):
+        """Ticks until every submitted request is done; returns their ids."""
+        done = []
+        while sum(self.pending()):
+            done += self.tick()
+        return done
+
+    def stats(self):
+        import json
+        buf = ctypes.create_string_buffer(1024)
+        check(lib().d3d_server_stats(self._h, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().d3d_server_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -33,13 +33,6 @@
 
 namespace d3d {
 
-struct BatchDesc {
-  float* a;
-  float* b;
-  int nx, ny, nz, tiles_x;
-  Coef<float> k;
-};
-
 template <int BX, int BY>
 struct BTile {
   static constexpr int THREADS = BX * BY;
@@ -147,15 +140,11 @@ __global__ void __launch_bounds__(256)
   const int bx = it.y % d.tiles_x, by = it.y / d.tiles_x;
   const float* src = parity ? d.b : d.a;
   float* dst = parity ? d.a : d.b;
-  march_tile<BX, BY>(src, dst, d.nx, d.ny, d.nz, bx * BX, by * BY, d.k,
-                     stage);
+  const Coef<float> k{d.k[0], d.k[1], d.k[2], d.k[3],
+                      d.k[4], d.k[5], d.k[6], d.k[7]};
+  march_tile<BX, BY>(src, dst, d.nx, d.ny, d.nz, bx * BX, by * BY, k, stage);
 }
 
-// Tile shapes the batch kernel is instantiated for.
-struct BShape {
-  int bx, by;
-};
-constexpr int kNumBShapes = 3;
 const BShape kBShapes[kNumBShapes] = {{32, 8}, {16, 16}, {64, 4}};
 
 cudaError_t launch_batch_step(int shape, const BatchDesc* descs,
@@ -253,8 +242,8 @@ int build_class(d3d_batch b, ClassPlan& c) {
     d.nz = g.nz;
     d.tiles_x = (g.nx + sh.bx - 1) / sh.bx;
     const int tiles = d.tiles_x * ((g.ny + sh.by - 1) / sh.by);
-    d.k = d3d::Coef<float>{g.coeff[0], g.coeff[1], g.coeff[2], g.coeff[3],
-                           g.coeff[4], g.coeff[5], g.coeff[6], -0.0f};
+    for (int j = 0; j < 7; ++j) d.k[j] = g.coeff[j];
+    d.k[7] = -0.0f;
     descs.push_back(d);
     for (int t = 0; t < tiles; ++t) items.push_back(make_int2((int)gi, t));
     // items of this grid are active for steps [0, g.steps)

@@ -83,6 +83,27 @@ cudaError_t launch_compare_noalloc(const void* a, int a_dtype, const void* b,
                                    int b_dtype, size_t n, double* scratch,
                                    cudaStream_t stream);
 
+// One grid of a multi-grid step launch: step `parity` reads a (parity 0)
+// or b (parity 1) and writes the other.
+struct BatchDesc {
+  float* a;
+  float* b;
+  int nx, ny, nz, tiles_x;
+  float k[8];  // ce, cw, cn, cs, ct, cb, cc, and -0.0
+};
+
+// Tile shapes of the multi-grid step kernel (256 threads each).
+struct BShape {
+  int bx, by;
+};
+constexpr int kNumBShapes = 3;
+extern const BShape kBShapes[kNumBShapes];
+
+// One time step for `nitems` (grid, tile) work items.
+cudaError_t launch_batch_step(int shape, const BatchDesc* descs,
+                              const int2* items, int nitems, int parity,
+                              cudaStream_t s);
+
 // Analytic solution (the reference's Initialize, computed in FP64 on the
 // device) written in `dtype` at `time`.
 cudaError_t launch_analytic(void* out, int dtype, int nx, int ny, int nz,

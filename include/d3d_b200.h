@@ -204,6 +204,51 @@ int d3d_batch_info(d3d_batch batch, char* buf, size_t len);
 
 int d3d_batch_destroy(d3d_batch batch);
 
+/* ---------------------------------------------------------------------
+ * Serving: a continuous-batching solve server.  No counterpart in the
+ * reference (a served request is what one RunKernel call does there:
+ * InitializeBenchmark -> RunKernel -> FinalizeBenchmark).
+ *
+ * Requests (grid shape, steps, coefficients, a host input field and a host
+ * output buffer) are queued by d3d_server_submit.  Each d3d_server_tick
+ *   1. retires solves whose result has reached host memory,
+ *   2. admits queued solves whose two buffers fit in the free part of the
+ *      server's device arena (its HBM budget), copying their inputs in on a
+ *      copy stream,
+ *   3. advances every active solve by up to `chunk` steps with the
+ *      multi-grid step kernel (solves admitted this tick included), and
+ *   4. starts the device->host copy of every solve that just finished.
+ * Requests that arrive while others run join at the next tick; their work
+ * overlaps on the device.  Each solve's arithmetic is RunKernel's, so its
+ * result is bit-identical whether it runs alone or in any mix.
+ * Host buffers must stay valid until the request is reported done; pinned
+ * buffers (d3d_host_alloc) make the copies asynchronous.
+ * --------------------------------------------------------------------- */
+typedef struct d3d_server_s* d3d_server;
+
+/* arena_bytes: device memory reserved for solve state (allocated once). */
+int d3d_server_create(size_t arena_bytes, int chunk, d3d_server* out);
+
+/* Queues one solve; *id receives its request id.  D3D_E_BUSY if the solve
+ * can never fit the arena (2 * nx*ny*nz floats > arena). */
+int d3d_server_submit(d3d_server server, int nx, int ny, int nz, int steps,
+                      const float coeff[7], const float* host_in,
+                      float* host_out, long long* id);
+
+/* One scheduling round (does not wait for the GPU except to keep at most
+ * two rounds in flight).  Writes up to max_done finished request ids. */
+int d3d_server_tick(d3d_server server, long long* done_ids, int max_done,
+                    int* n_done);
+
+/* Number of requests queued, active on the device and copying out. */
+int d3d_server_pending(d3d_server server, int* queued, int* active,
+                       int* retiring);
+
+/* JSON counters: submitted, completed, ticks, launches, peak arena use. */
+int d3d_server_stats(d3d_server server, char* buf, size_t len);
+
+int d3d_server_destroy(d3d_server server);
+
 /* d3d_compare without any device allocation.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory at
  * the moment they want an error report -- a serving loop that has already

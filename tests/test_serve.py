@@ -1,0 +1,93 @@
+"""The continuous-batching server (d3d_server_*): every served result must be
+bit-identical to the oracle's RunKernel, whether the request runs alone or
+in a mix, arrives while others are on the GPU, or waits for arena space."""
+import numpy as np
+import pytest
+
+import benchmarks_b200 as B
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(seed, n, max_side=48, max_steps=40, cubic=False):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(n):
+        if cubic:
+            nx = ny = nz = int(rng.integers(4, max_side + 1))
+        else:
+            nx, ny, nz = (int(v) for v in rng.integers(1, max_side + 1, 3))
+        steps = int(rng.integers(0, max_steps + 1))
+        c = B.batch_coefficients(nx, ny, nz, float(rng.uniform(0.05, 0.2)))
+        f = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), seed + i)
+        reqs.append((f, steps, c))
+    return reqs
+
+
+def _serve(reqs, arena_bytes=1 << 28, chunk=8, interleave=False):
+    server = B.Server(arena_bytes, chunk)
+    outs = [np.full_like(f, np.nan) for f, _, _ in reqs]
+    ids = {}
+    done = set()
+    for k, ((f, steps, c), o) in enumerate(zip(reqs, outs)):
+        ids[server.submit(f, o, steps, c)] = k
+        if interleave and k % 3 == 2:
+            done.update(server.tick())  # others are running meanwhile
+    done.update(server.drain())
+    assert done == set(ids)
+    stats = server.stats()
+    server.close()
+    return outs, stats
+
+
+def test_served_results_bit_exact_vs_oracle():
+    reqs = _requests(1, 30)
+    outs, stats = _serve(reqs)
+    for (f, steps, c), o in zip(reqs, outs):
+        assert o.tobytes() == O.run(f, c, steps).tobytes()
+    assert stats["completed"] == len(reqs)
+
+
+def test_same_alone_and_in_the_mix():
+    reqs = _requests(2, 18, max_side=40, max_steps=30)
+    mixed, _ = _serve(reqs, interleave=True)
+    for k in (0, 4, 9, 17):
+        alone, _ = _serve([reqs[k]])
+        assert alone[0].tobytes() == mixed[k].tobytes()
+
+
+@pytest.mark.parametrize("chunk", [1, 3, 16])
+def test_chunk_sizes_and_late_arrivals(chunk):
+    reqs = _requests(3, 15, max_side=32, max_steps=25)
+    outs, stats = _serve(reqs, chunk=chunk, interleave=True)
+    for (f, steps, c), o in zip(reqs, outs):
+        assert o.tobytes() == O.run(f, c, steps).tobytes()
+    assert stats["chunk"] == chunk
+
+
+def test_small_arena_queues_until_space_frees():
+    # Room for about one 40^3 solve at a time: admission must wait.
+    reqs = _requests(4, 8, max_side=40, max_steps=12, cubic=True)
+    arena = 2 * 4 * 40 ** 3 + 4096
+    outs, stats = _serve(reqs, arena_bytes=arena)
+    for (f, steps, c), o in zip(reqs, outs):
+        assert o.tobytes() == O.run(f, c, steps).tobytes()
+    assert stats["peak_arena_bytes"] <= arena
+
+
+def test_rejects_solves_that_can_never_fit():
+    server = B.Server(1 << 20)
+    f = np.zeros((64, 64, 64), np.float32)  # 2 x 1 MiB > 1 MiB arena
+    o = np.zeros_like(f)
+    with pytest.raises(B.D3DError) as ei:
+        server.submit(f, o, 3, O.params(64, 64, 64)[0])
+    assert ei.value.code == B.D3D_E_BUSY
+    server.close()
+
+
+def test_zero_step_requests_return_their_input():
+    reqs = [(O.seeded_noise((5, 6, 7), 1, amplitude=1.0), 0,
+             O.params(7, 6, 5)[0])]
+    outs, _ = _serve(reqs)
+    assert outs[0].tobytes() == reqs[0][0].tobytes()
