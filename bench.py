@@ -161,6 +161,128 @@ def cpu_reference_leg(n_side, steps_hint=None, budget_s=12.0):
                           else "oracle port", t)}
 
 
+def batched_leg(B, torch, n_grids=4096, plain_sample=64):
+    """Config: 4096 grids, sides U{16..96} per axis, kappa U[0.05,0.2],
+    steps U{10..500}; one batched run (one CUDA graph) vs a plain per-solve
+    loop (a plan, two device buffers and a RunKernel-style d3d_run per
+    grid) on the first `plain_sample` grids."""
+    from benchmarks_b200.workloads import batched_specs
+    specs = batched_specs(n_grids)
+    updates = sum(nx * ny * nz * s for nx, ny, nz, s, _ in specs)
+    batch = B.Batch(specs)
+    batch.autotune()
+    batch.arena.uniform_(0.0, 1.0)
+    batch.run()  # capture + first replay
+    runs = [batch.run() for _ in range(3)]
+    ms = min(runs)
+    info = batch.info()
+    batch.close()
+    del batch
+    torch.cuda.empty_cache()
+    sample = specs[:plain_sample]
+    upd_s = sum(nx * ny * nz * s for nx, ny, nz, s, _ in sample)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for (nx, ny, nz, s, c) in sample:
+        p = B.Plan(nx, ny, nz)
+        p.set_graphs(False)
+        f1 = p.empty()
+        f2 = p.empty()
+        p.run(f1, f2, s, c)
+        torch.cuda.synchronize()
+        p.close()
+    t_plain = time.perf_counter() - t0
+    plain_solves = len(sample) / t_plain
+    solves = n_grids / (ms / 1e3)
+    return {"grids": n_grids, "updates": updates, "ms": ms,
+            "solves_per_s": solves, "value": updates / (ms / 1e3) / 1e9,
+            "unit": UNIT, "launches_per_run": info["launches_per_run"],
+            "tiles": [c["tile"] for c in info["classes"]],
+            "plain_loop": {"sample_grids": len(sample),
+                           "solves_per_s": plain_solves,
+                           "value": upd_s / t_plain / 1e9},
+            "speedup_solves": solves / plain_solves}
+
+
+def serving_leg(B, torch, n_req=96, arena_gb=24.0, chunk=8):
+    """Config: Poisson stream (mean 2000 req/s) of cubic FP32 solves, sides
+    log-uniform in [32, 256], steps log-uniform in [10, 2000]; the
+    continuous-batching server vs a plain per-request loop (allocate,
+    RunKernel with host copies, free) over the same arrivals.  Latency is
+    completion time minus scheduled arrival."""
+    from benchmarks_b200.workloads import serving_requests
+    reqs = serving_requests(n_req)
+    sizes = [s ** 3 for _, s, _ in reqs]
+    maxn = max(sizes)
+    pool_in = torch.rand(maxn, pin_memory=True).numpy()
+    out_pool = torch.empty(sum(sizes), pin_memory=True).numpy()
+    offs = np.cumsum([0] + sizes[:-1])
+    coeff = {}
+    for _, s, _ in reqs:
+        if s not in coeff:
+            coeff[s] = B.coefficients(s, s, s)[0]
+    upd = sum(n * st for n, (_, _, st) in zip(sizes, reqs))
+
+    def lat_stats(done_at):
+        lat = np.array([done_at[i] - reqs[i][0] for i in range(n_req)])
+        span = max(done_at) - reqs[0][0]
+        return {"solves_per_s": n_req / span, "p50_ms": 1e3 * float(
+            np.percentile(lat, 50)), "p99_ms": 1e3 * float(
+            np.percentile(lat, 99)), "makespan_s": span,
+            "value": upd / span / 1e9}
+
+    # served
+    server = B.Server(int(arena_gb * 2 ** 30), chunk)
+    done_at = [0.0] * n_req
+    idmap = {}
+    nxt = 0
+    t0 = time.perf_counter()
+    while len(idmap) < n_req or sum(server.pending()):
+        now = time.perf_counter() - t0
+        while nxt < n_req and reqs[nxt][0] <= now:
+            _, s, st = reqs[nxt]
+            hin = pool_in[:s ** 3].reshape(s, s, s)
+            hout = out_pool[offs[nxt]:offs[nxt] + s ** 3].reshape(s, s, s)
+            idmap[server.submit(hin, hout, st, coeff[s])] = nxt
+            nxt += 1
+        for rid in server.tick():
+            done_at[idmap[rid]] = time.perf_counter() - t0
+        if nxt < n_req and not sum(server.pending()):
+            time.sleep(max(0.0, reqs[nxt][0] - (time.perf_counter() - t0)))
+    served = lat_stats(done_at)
+    served["stats"] = server.stats()
+    server.close()
+    # plain per-request loop
+    import ctypes
+    done_at = [0.0] * n_req
+    t0 = time.perf_counter()
+    for i, (arr, s, st) in enumerate(reqs):
+        now = time.perf_counter() - t0
+        if arr > now:
+            time.sleep(arr - now)
+        n = s ** 3
+        p = B.Plan(s, s, s)
+        p.set_graphs(False)
+        d1, d2 = ctypes.c_void_p(), ctypes.c_void_p()
+        B.check(B.lib().d3d_device_alloc(n * 4, ctypes.byref(d1)))
+        B.check(B.lib().d3d_device_alloc(n * 4, ctypes.byref(d2)))
+        host = out_pool[offs[i]:offs[i] + n]
+        host[:] = pool_in[:n]
+        ms = ctypes.c_float()
+        B.check(B.lib().d3d_run_host(p.handle, host.ctypes.data, d1, d2,
+                                     coeff[s].ctypes.data, st, None,
+                                     ctypes.byref(ms)))
+        B.lib().d3d_device_free(d1)
+        B.lib().d3d_device_free(d2)
+        p.close()
+        done_at[i] = time.perf_counter() - t0
+    plain = lat_stats(done_at)
+    return {"requests": n_req, "rate_per_s": 2000.0, "updates": upd,
+            "unit": UNIT, "served": served, "plain_loop": plain,
+            "speedup_solves": served["solves_per_s"] / plain["solves_per_s"],
+            "p99_ratio_plain_over_served": plain["p99_ms"] / served["p99_ms"]}
+
+
 def run_reference_arm(args):
     rank, world, _ = env_rank()
     if rank != 0:
@@ -381,6 +503,12 @@ def run_b200(args):
         "correctness": report,
         "side": side,
     }
+    if not args.no_side:
+        del a, b, f1, f2, host
+        torch.cuda.empty_cache()
+        side["batched"] = batched_leg(B, torch)
+        torch.cuda.empty_cache()
+        side["serving"] = serving_leg(B, torch)
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_reference_leg(n)
     if rank == 0:
@@ -398,6 +526,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true",
                     help="skip the CPU baseline leg")
+    ap.add_argument("--no-side", action="store_true",
+                    help="skip the batched and serving legs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
