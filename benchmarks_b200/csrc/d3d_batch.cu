@@ -12,15 +12,9 @@
 // contributes one work item per xy tile, so the items still active at step
 // s are a prefix of the class's list: step s launches exactly that prefix.
 //
-// Tile kernel (march_tile).  A CTA marches its tile through all nz planes.
-// Each thread owns its interior cell and at most one halo cell, and keeps
-// the next P planes of both in a register queue (loads in flight), stores
-// the current plane into one of two shared halo planes (one __syncthreads
-// per plane), takes n/s/w/e from shared memory and b/c/t from its queue.
-// Every load address is clamped into the grid, which is exactly the
-// reference's replicated-neighbour boundary, so no value is ever selected.
-// Each point is d3d::point: results are bit-identical to running each grid
-// alone.
+// Tile kernel: d3d::march_tile (d3d_march.cuh) over all nz planes of the
+// item's grid.  Each point is d3d::point: results are bit-identical to
+// running each grid alone.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -30,111 +24,15 @@
 #include "d3d_b200.h"
 #include "d3d_common.cuh"
 #include "d3d_kernels.h"
+#include "d3d_march.cuh"
 
 namespace d3d {
-
-template <int BX, int BY>
-struct BTile {
-  static constexpr int THREADS = BX * BY;
-  static constexpr int W = BX + 2;
-  static constexpr int H = BY + 2;
-  static constexpr int E = W * H;
-  static constexpr int HALO = E - BX * BY;
-  static_assert(THREADS == 256, "tile kernels run 256 threads");
-  static_assert(HALO <= THREADS, "one halo cell per thread at most");
-};
-
-constexpr int kQ = 4;  // planes in each thread's register queue
-
-// One plane's loads for this thread: its interior cell and its halo cell.
-struct Pair {
-  float own, halo;
-};
-
-template <int BX, int BY>
-__device__ __forceinline__ void march_tile(const float* __restrict__ src,
-                                           float* __restrict__ dst, int nx,
-                                           int ny, int nz, int x0, int y0,
-                                           const Coef<float>& k,
-                                           float (*stage)[BTile<BX, BY>::E]) {
-  using TL = BTile<BX, BY>;
-  const int tid = threadIdx.x;
-  const int tx = tid % BX, ty = tid / BX;
-  const int xg = x0 + tx, yg = y0 + ty;
-  // Interior cell: stage index and clamped in-plane offset.
-  const int own_s = (ty + 1) * TL::W + (tx + 1);
-  const int own_g = min(yg, ny - 1) * nx + min(xg, nx - 1);
-  // Halo cell h = tid (if any): the border of the W x H box.
-  const bool has_halo = tid < TL::HALO;
-  int lx = 0, ly = 0;
-  {
-    const int h = tid;
-    if (h < TL::W) {
-      lx = h;
-      ly = 0;
-    } else if (h < 2 * TL::W) {
-      lx = h - TL::W;
-      ly = TL::H - 1;
-    } else if (h < 2 * TL::W + TL::H - 2) {
-      lx = 0;
-      ly = 1 + h - 2 * TL::W;
-    } else {
-      lx = TL::W - 1;
-      ly = 1 + h - 2 * TL::W - (TL::H - 2);
-    }
-  }
-  const int halo_s = ly * TL::W + lx;
-  const int hx = min(max(x0 - 1 + lx, 0), nx - 1);
-  const int hy = min(max(y0 - 1 + ly, 0), ny - 1);
-  const int halo_g = hy * nx + hx;
-  const bool store_ok = xg < nx && yg < ny;
-  const size_t plane = (size_t)nx * ny;
-
-  auto load = [&](int p) -> Pair {
-    const float* pl = src + (size_t)min(p, nz - 1) * plane;
-    Pair v;
-    v.own = __ldg(pl + own_g);
-    v.halo = has_halo ? __ldg(pl + halo_g) : 0.0f;
-    return v;
-  };
-
-  Pair q0 = load(0), q1 = load(1), q2 = load(2), q3 = load(3);
-  float b = q0.own;  // plane -1 is plane 0
-
-  // One plane: publish `cur`, refill its slot with plane z+kQ, compute.
-  auto plane_step = [&](int z, Pair& cur, const Pair& next) {
-    float* st = stage[z & 1];
-    st[own_s] = cur.own;
-    if (has_halo) st[halo_s] = cur.halo;
-    const float c = cur.own;
-    const float t = next.own;  // plane min(z+1, nz-1)
-    cur = load(z + kQ);
-    __syncthreads();
-    const float w = st[own_s - 1];
-    const float e = st[own_s + 1];
-    const float n = st[own_s - TL::W];
-    const float s = st[own_s + TL::W];
-    const float v = point(k, c, w, e, s, n, b, t);
-    if (store_ok) dst[(size_t)z * plane + (size_t)yg * nx + xg] = v;
-    b = c;
-  };
-
-  for (int z = 0; z < nz; z += kQ) {
-    plane_step(z, q0, q1);
-    if (z + 1 >= nz) break;
-    plane_step(z + 1, q1, q2);
-    if (z + 2 >= nz) break;
-    plane_step(z + 2, q2, q3);
-    if (z + 3 >= nz) break;
-    plane_step(z + 3, q3, q0);
-  }
-}
 
 template <int BX, int BY>
 __global__ void __launch_bounds__(256)
     batch_step_kernel(const BatchDesc* __restrict__ descs,
                       const int2* __restrict__ items, int parity) {
-  __shared__ float stage[2][BTile<BX, BY>::E];
+  __shared__ float stage[2][MarchTile<BX, BY>::E];
   const int2 it = items[blockIdx.x];
   const BatchDesc d = descs[it.x];
   const int bx = it.y % d.tiles_x, by = it.y / d.tiles_x;
@@ -142,7 +40,8 @@ __global__ void __launch_bounds__(256)
   float* dst = parity ? d.a : d.b;
   const Coef<float> k{d.k[0], d.k[1], d.k[2], d.k[3],
                       d.k[4], d.k[5], d.k[6], d.k[7]};
-  march_tile<BX, BY>(src, dst, d.nx, d.ny, d.nz, bx * BX, by * BY, k, stage);
+  march_tile<float, BX, BY>(src, dst, d.nx, d.ny, d.nz, bx * BX, by * BY, 0,
+                            d.nz, k, stage);
 }
 
 const BShape kBShapes[kNumBShapes] = {{32, 8}, {16, 16}, {64, 4}};

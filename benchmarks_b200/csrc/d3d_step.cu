@@ -15,8 +15,8 @@
 //    is a 128-bit coalesced store.
 //
 //  * step_generic_kernel -- any shape and alignment (TMA needs 16-byte row
-//    pitches): 32x8 tiles, halo cells fetched with clamped coordinates so
-//    the replicated boundary falls out of the addressing.
+//    pitches): d3d::march_tile over 32x8 tiles and z-chunks, clamped load
+//    addresses implementing the replicated boundary.
 //
 // Both evaluate d3d::point (exact reference order, no FMA), so results are
 // bit-identical to Diffusion3DOpenMP::RunKernel.
@@ -25,6 +25,7 @@
 
 #include "d3d_common.cuh"
 #include "d3d_kernels.h"
+#include "d3d_march.cuh"
 
 namespace d3d {
 
@@ -213,64 +214,22 @@ drain:
 }
 
 // ---------------------------------------------------------------------------
-// Generic kernel: any nx, ny, nz, any alignment.
+// Generic kernel: any nx, ny, nz, any alignment -- d3d::march_tile over a
+// 32 x 8 tile and a z-chunk (d3d_march.cuh).
 // ---------------------------------------------------------------------------
 constexpr int kGenBX = 32;
 constexpr int kGenBY = 8;
 
 template <typename T>
-__global__ void __launch_bounds__(kGenBX* kGenBY)
+__global__ void __launch_bounds__(256)
     step_generic_kernel(const T* __restrict__ src, T* __restrict__ dst,
                         int nx, int ny, int nz, Coef<T> k, int zchunk) {
-  __shared__ T tile[kGenBY + 2][kGenBX + 2];
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int xg = blockIdx.x * kGenBX + tx;
-  const int yg = blockIdx.y * kGenBY + ty;
+  __shared__ T stage[2][MarchTile<kGenBX, kGenBY>::E];
   const int z0 = blockIdx.z * zchunk;
   const int z1 = min(nz, z0 + zchunk);
   if (z0 >= z1) return;
-  // Clamped coordinates: out-of-domain halo cells read the edge cell, which
-  // is exactly the reference's replicated-neighbour rule.
-  const int xc = min(xg, nx - 1);
-  const int yc = min(yg, ny - 1);
-  const size_t xy = (size_t)nx * ny;
-  const T* col = src + (size_t)yc * nx + xc;
-  const bool edge_w = (tx == 0), edge_e = (tx == kGenBX - 1);
-  const bool edge_n = (ty == 0), edge_s = (ty == kGenBY - 1);
-  const int xw = max(xg - 1, 0), xe = min(xg + 1, nx - 1);
-  const int yn = max(yg - 1, 0), ys = min(yg + 1, ny - 1);
-  const int xwc = min(xw, nx - 1), xec = min(xe, nx - 1);
-  const int ync = min(yn, ny - 1), ysc = min(ys, ny - 1);
-
-  T b = __ldg(col + (size_t)max(z0 - 1, 0) * xy);
-  T c = __ldg(col + (size_t)z0 * xy);
-  for (int z = z0; z < z1; ++z) {
-    const T t = __ldg(col + (size_t)min(z + 1, nz - 1) * xy);
-    const T* plane = src + (size_t)z * xy;
-    tile[ty + 1][tx + 1] = c;
-    if (edge_w) tile[ty + 1][0] = __ldg(plane + (size_t)yc * nx + xwc);
-    if (edge_e) tile[ty + 1][kGenBX + 1] = __ldg(plane + (size_t)yc * nx + xec);
-    if (edge_n) tile[0][tx + 1] = __ldg(plane + (size_t)ync * nx + xc);
-    if (edge_s) tile[kGenBY + 1][tx + 1] = __ldg(plane + (size_t)ysc * nx + xc);
-    __syncthreads();
-    // Inside the tile the neighbour cell is the tile cell; at a domain
-    // edge the clamped load above already holds the centre value.  A tile
-    // cell beyond the domain (xg >= nx) holds a clamped copy, and only
-    // feeds outputs that are not stored.
-    T w = tile[ty + 1][tx];
-    T e = tile[ty + 1][tx + 2];
-    T n = tile[ty][tx + 1];
-    T s = tile[ty + 2][tx + 1];
-    if (xg == 0) w = c;
-    if (xg == nx - 1) e = c;
-    if (yg == 0) n = c;
-    if (yg == ny - 1) s = c;
-    const T v = point(k, c, w, e, s, n, b, t);
-    if (xg < nx && yg < ny) dst[(size_t)z * xy + (size_t)yg * nx + xg] = v;
-    __syncthreads();
-    b = c;
-    c = t;
-  }
+  march_tile<T, kGenBX, kGenBY>(src, dst, nx, ny, nz, blockIdx.x * kGenBX,
+                                blockIdx.y * kGenBY, z0, z1, k, stage);
 }
 
 // ---------------------------------------------------------------------------
@@ -425,10 +384,10 @@ cudaError_t launch_step_generic(const void* f1, void* f2, int nx, int ny,
                                 cudaStream_t stream, LaunchInfo* info) {
   const int gx = (nx + kGenBX - 1) / kGenBX;
   const int gy = (ny + kGenBY - 1) / kGenBY;
-  const int zchunk = pick_zchunk(nz, (long)gx * gy, 8, 8);
+  const int zchunk = pick_zchunk(nz, (long)gx * gy, 8, 32);
   const int gz = (nz + zchunk - 1) / zchunk;
   if (info) *info = LaunchInfo{gx, gy, gz, kGenBX * kGenBY, 0, zchunk, 8};
-  dim3 grid(gx, gy, gz), block(kGenBX, kGenBY);
+  dim3 grid(gx, gy, gz), block(kGenBX * kGenBY);
   if (dtype == kF64)
     step_generic_kernel<double><<<grid, block, 0, stream>>>(
         static_cast<const double*>(f1), static_cast<double*>(f2), nx, ny, nz,
