@@ -503,7 +503,7 @@ def run_b200(args):
         "correctness": report,
         "side": side,
     }
-    if not args.no_side:
+    if not args.no_side and world == 1:
         del a, b, f1, f2, host
         torch.cuda.empty_cache()
         side["batched"] = batched_leg(B, torch)

@@ -1,0 +1,138 @@
+"""Multi-rank paths on CPU (gloo, 127.0.0.1), no GPU needed.
+
+* z-slab decomposition with halo exchange: ranks run the oracle's step on
+  their local slab (the CUDA kernels take that role on GPUs); the gathered
+  field must be bit-identical to a single-process run, for several world
+  sizes, halo depths and uneven slabs.
+* bench-style max-over-ranks timing reduction.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from benchmarks_b200.distributed import SlabDecomposition, slab_bounds
+
+
+def test_slab_bounds_cover_the_grid():
+    for nz in (5, 16, 17, 100):
+        for world in range(1, 6):
+            if world > nz:
+                continue
+            spans = [slab_bounds(nz, r, world) for r in range(world)]
+            assert spans[0][0] == 0 and spans[-1][1] == nz
+            for (a0, a1), (b0, b1) in zip(spans, spans[1:]):
+                assert a1 == b0
+            sizes = [z1 - z0 for z0, z1 in spans]
+            assert max(sizes) - min(sizes) <= 1
+
+
+def test_decomposition_slices():
+    d = SlabDecomposition(20, 1, 3, halo=2)  # owns [7, 14)
+    assert (d.z0, d.z1, d.lo, d.hi) == (7, 14, 5, 16)
+    assert d.owned() == slice(2, 9)
+    assert d.send_down() == slice(2, 4) and d.recv_down() == slice(0, 2)
+    assert d.send_up() == slice(7, 9) and d.recv_up() == slice(9, 11)
+    edge = SlabDecomposition(20, 0, 3, halo=2)
+    assert edge.lo == 0 and edge.down is None and edge.recv_down() == slice(0, 0)
+    with pytest.raises(ValueError):
+        SlabDecomposition(4, 0, 3, halo=3)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _slab_worker(rank, world, port, nx, ny, nz, count, halo, seed, out):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    import oracle as O
+    from benchmarks_b200.distributed import SlabSolver
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=timedelta(seconds=60))
+    try:
+        c, _ = O.params(nx, ny, nz)
+        field = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), seed)
+        lib = O.lib()
+
+        def step(src, dst):  # the oracle's step on the local slab
+            s = src.numpy()
+            d = dst.numpy()
+            lib.d3do_step_f32(s.ctypes.data_as(O._f32p),
+                              d.ctypes.data_as(O._f32p), nx, ny, s.shape[0],
+                              c.ctypes.data_as(O._f32p))
+
+        solver = SlabSolver(dist, nx, ny, nz, c, halo=halo, step_fn=step,
+                            device=torch.device("cpu"))
+        solver.load(torch.from_numpy(field))
+        solver.run(count)
+        full = solver.gather().numpy()
+        # max-over-ranks reduction as bench.py does it
+        t = torch.tensor([float(rank + 1)], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        if rank == 0:
+            np.save(out, full)
+            assert t.item() == world
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,halo,dims,count", [
+    (2, 1, (12, 9, 16), 7),
+    (2, 3, (10, 7, 15), 8),
+    (3, 2, (8, 8, 17), 11),
+    (3, 1, (5, 6, 7), 5),
+])
+def test_slab_solver_matches_single_process(tmp_path, world, halo, dims,
+                                            count):
+    import torch.multiprocessing as mp
+
+    import oracle as O
+    nx, ny, nz = dims
+    out = str(tmp_path / "full.npy")
+    mp.start_processes(_slab_worker,
+                       args=(world, _free_port(), nx, ny, nz, count, halo, 5,
+                             out),
+                       nprocs=world, join=True, start_method="spawn")
+    full = np.load(out)
+    c, _ = O.params(nx, ny, nz)
+    field = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), 5)
+    assert full.tobytes() == O.run(field, c, count).tobytes()
+
+
+@pytest.mark.gpu
+def test_slab_solver_cuda_kernels_world_one():
+    """The default step (our CUDA kernels through the C ABI) inside the slab
+    solver, on one GPU with an NCCL group of one."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    import oracle as O
+    from benchmarks_b200.distributed import SlabSolver
+
+    nx, ny, nz, count = 64, 40, 36, 9
+    c, _ = O.params(nx, ny, nz)
+    field = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), 2)
+    store = dist.TCPStore("127.0.0.1", _free_port(), 1, True)
+    dist.init_process_group("nccl", store=store, rank=0, world_size=1,
+                            timeout=timedelta(seconds=60))
+    try:
+        solver = SlabSolver(dist, nx, ny, nz, c, halo=2)
+        solver.load(torch.from_numpy(field).cuda())
+        solver.run(count)
+        torch.cuda.synchronize()
+        full = solver.gather().cpu().numpy()
+    finally:
+        dist.destroy_process_group()
+    assert full.tobytes() == O.run(field, c, count).tobytes()
