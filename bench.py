@@ -426,11 +426,15 @@ def run_b200(args):
     side = {}
     for k in (2, 3, 4):
         ptb = B.Plan(n, n, n, B.F32, B.KERNEL_TB, k)
-        r, inf = rate_of(ptb, a, b, 3)
+        ptb.autotune(a, b, steps=4 * k, coeff=coeff, stream=stream)
+        r, _ = rate_of(ptb, a, b, 3)
+        a, b = ptb.run(a, b, k, coeff, stream)  # one fused pass: its geometry
+        inf = ptb.info()
         side["tb%d" % k] = {
             "value": r, "unit": UNIT,
             "effective_hbm_frac": r * 1e9 * BYTES_PER_UPDATE / (peak * 1e9),
-            "grid": inf["grid"], "smem": inf["smem"]}
+            "kernel": inf["last_kernel"], "grid": inf["grid"],
+            "zchunk": inf["launch_zchunk"], "smem": inf["smem"]}
         ptb.close()
 
     # --- correctness report: FP32 vs FP64 vs analytic, FP64 norms -------
