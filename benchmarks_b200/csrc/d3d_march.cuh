@@ -70,45 +70,63 @@ __device__ __forceinline__ void march_tile(const T* __restrict__ src,
   const bool store_ok = xg < nx && yg < ny;
   const size_t plane = (size_t)nx * ny;
 
-  auto load = [&](int p) -> MarchPair<T> {
-    const T* pl = src + (size_t)min(p, nz - 1) * plane;
+  // Load pointers step one plane per call and stop at the last plane the
+  // chunk needs (plane z1 is the t of plane z1-1); later calls re-read it.
+  const int plim = min(z1, nz - 1);
+  int pn = z0;  // plane the next load reads
+  const T* po = src + (size_t)z0 * plane + own_g;
+  const T* ph = src + (size_t)z0 * plane + halo_g;
+  auto load_next = [&]() -> MarchPair<T> {
     MarchPair<T> v;
-    v.own = __ldg(pl + own_g);
-    v.halo = has_halo ? __ldg(pl + halo_g) : T(0);
+    v.own = __ldg(po);
+    v.halo = has_halo ? __ldg(ph) : T(0);
+    if (pn < plim) {
+      po += plane;
+      ph += plane;
+    }
+    ++pn;
     return v;
   };
 
-  MarchPair<T> q0 = load(z0), q1 = load(min(z0 + 1, z1)),
-               q2 = load(min(z0 + 2, z1)), q3 = load(min(z0 + 3, z1));
+  MarchPair<T> q[kMarchQ];
+#pragma unroll
+  for (int i = 0; i < kMarchQ; ++i) q[i] = load_next();
   // b of the first plane: plane z0-1, or plane 0 itself at the bottom.
-  T b = (z0 > 0) ? __ldg(src + (size_t)(z0 - 1) * plane + own_g) : q0.own;
+  T b = (z0 > 0) ? __ldg(src + (size_t)(z0 - 1) * plane + own_g) : q[0].own;
+  T* out = dst + (size_t)z0 * plane + (size_t)min(yg, ny - 1) * nx +
+           min(xg, nx - 1);
 
-  // One plane: publish `cur`, refill its slot with plane z+kQ, compute.
-  auto plane_step = [&](int z, MarchPair<T>& cur, const MarchPair<T>& next) {
-    T* st = stage[z & 1];
+  // One plane: publish `cur` into stage `st`, refill the slot with the next
+  // plane in line, compute, store.
+  auto plane_step = [&](T* st, MarchPair<T>& cur, const MarchPair<T>& next) {
     st[own_s] = cur.own;
     if (has_halo) st[halo_s] = cur.halo;
     const T c = cur.own;
     const T t = next.own;  // plane min(z+1, nz-1)
-    cur = load(min(z + kMarchQ, z1));  // past the chunk: plane z1 again
+    cur = load_next();
     __syncthreads();
     const T w = st[own_s - 1];
     const T e = st[own_s + 1];
     const T n = st[own_s - TL::W];
     const T s = st[own_s + TL::W];
     const T v = point(k, c, w, e, s, n, b, t);
-    if (store_ok) dst[(size_t)z * plane + (size_t)yg * nx + xg] = v;
+    if (store_ok) *out = v;
+    out += plane;
     b = c;
   };
 
+  // Unrolled kMarchQ (even) ways: queue slots and stage parity are
+  // compile-time constants, so the queue stays in registers.
   for (int z = z0; z < z1; z += kMarchQ) {
-    plane_step(z, q0, q1);
-    if (z + 1 >= z1) break;
-    plane_step(z + 1, q1, q2);
-    if (z + 2 >= z1) break;
-    plane_step(z + 2, q2, q3);
-    if (z + 3 >= z1) break;
-    plane_step(z + 3, q3, q0);
+    bool more = true;
+#pragma unroll
+    for (int i = 0; i < kMarchQ; ++i) {
+      if (more) {
+        plane_step(stage[i & 1], q[i], q[(i + 1) % kMarchQ]);
+        more = (z + i + 1 < z1);
+      }
+    }
+    if (!more) break;
   }
 }
 
