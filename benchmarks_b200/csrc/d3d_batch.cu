@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstring>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 #include "d3d_b200.h"
@@ -28,11 +29,15 @@
 
 namespace d3d {
 
-template <int BX, int BY>
+// PAIR: two cells per thread with packed arithmetic (march_tile2);
+// otherwise one cell per thread (march_tile).
+template <int BX, int BY, bool PAIR>
 __global__ void __launch_bounds__(256)
     batch_step_kernel(const BatchDesc* __restrict__ descs,
                       const int2* __restrict__ items, int parity) {
-  __shared__ float stage[2][MarchTile<BX, BY>::E];
+  using TileT =
+      std::conditional_t<PAIR, MarchTile2<BX, BY>, MarchTile<BX, BY>>;
+  __shared__ __align__(16) float stage[2][TileT::E];
   const int2 it = items[blockIdx.x];
   const BatchDesc d = descs[it.x];
   const int bx = it.y % d.tiles_x, by = it.y / d.tiles_x;
@@ -40,20 +45,28 @@ __global__ void __launch_bounds__(256)
   float* dst = parity ? d.a : d.b;
   const Coef<float> k{d.k[0], d.k[1], d.k[2], d.k[3],
                       d.k[4], d.k[5], d.k[6], d.k[7]};
-  march_tile<float, BX, BY>(src, dst, d.nx, d.ny, d.nz, bx * BX, by * BY, 0,
-                            d.nz, k, stage);
+  if constexpr (PAIR)
+    march_tile2<BX, BY>(src, dst, d.nx, d.ny, d.nz, bx * BX, by * BY, 0,
+                        d.nz, k, stage);
+  else
+    march_tile<float, BX, BY>(src, dst, d.nx, d.ny, d.nz, bx * BX, by * BY,
+                              0, d.nz, k, stage);
 }
 
-const BShape kBShapes[kNumBShapes] = {{32, 8}, {16, 16}, {64, 4}};
+// Shape 0 (32 x 16 cells as x-pairs) is the default, the autotuner's pick
+// for every size class of the 16..96 batch on B200; it may pick another per
+// class.
+const BShape kBShapes[kNumBShapes] = {{32, 16}, {64, 8}, {32, 8}, {16, 16}};
 
 cudaError_t launch_batch_step(int shape, const BatchDesc* descs,
                               const int2* items, int nitems, int parity,
                               cudaStream_t s) {
   if (nitems <= 0) return cudaSuccess;
   switch (shape) {
-    case 0: batch_step_kernel<32, 8><<<nitems, 256, 0, s>>>(descs, items, parity); break;
-    case 1: batch_step_kernel<16, 16><<<nitems, 256, 0, s>>>(descs, items, parity); break;
-    case 2: batch_step_kernel<64, 4><<<nitems, 256, 0, s>>>(descs, items, parity); break;
+    case 0: batch_step_kernel<32, 16, true><<<nitems, 256, 0, s>>>(descs, items, parity); break;
+    case 1: batch_step_kernel<64, 8, true><<<nitems, 256, 0, s>>>(descs, items, parity); break;
+    case 2: batch_step_kernel<32, 8, false><<<nitems, 256, 0, s>>>(descs, items, parity); break;
+    case 3: batch_step_kernel<16, 16, false><<<nitems, 256, 0, s>>>(descs, items, parity); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -96,7 +96,7 @@ struct BatchDesc {
 struct BShape {
   int bx, by;
 };
-constexpr int kNumBShapes = 3;
+constexpr int kNumBShapes = 4;
 extern const BShape kBShapes[kNumBShapes];
 
 // One time step for `nitems` (grid, tile) work items.

@@ -130,4 +130,128 @@ __device__ __forceinline__ void march_tile(const T* __restrict__ src,
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// FP32, two cells per thread: the same march with each thread owning an
+// x-pair, so the stencil runs on packed f32x2 pairs (point2, exact) and the
+// n/s neighbours are 8-byte shared loads.  The stage carries a two-column
+// left pad (column c <-> x = x0 - 2 + c) so every thread's pair is 8-byte
+// aligned; only columns 1 .. BX+2 are ever read.
+// ---------------------------------------------------------------------------
+template <int BX, int BY>
+struct MarchTile2 {
+  static constexpr int TX = BX / 2;  // threads per row
+  static constexpr int THREADS = TX * BY;
+  static constexpr int W = BX + 4;
+  static constexpr int H = BY + 2;
+  static constexpr int E = W * H;
+  static constexpr int HALO = 2 * (BX + 2) + 2 * BY;
+  static_assert(BX % 2 == 0, "pairs");
+  static_assert(THREADS == 256, "tile marches run 256 threads");
+  static_assert(HALO <= THREADS, "one halo cell per thread at most");
+};
+
+struct MarchQuad {
+  float o0, o1, halo;
+};
+
+template <int BX, int BY>
+__device__ __forceinline__ void march_tile2(
+    const float* __restrict__ src, float* __restrict__ dst, int nx, int ny,
+    int nz, int x0, int y0, int z0, int z1, const Coef<float>& k,
+    float (*stage)[MarchTile2<BX, BY>::E]) {
+  using TL = MarchTile2<BX, BY>;
+  const int tid = threadIdx.x;
+  const int tx = tid % TL::TX, ty = tid / TL::TX;
+  const int xg = x0 + 2 * tx, yg = y0 + ty;
+  const int own_s = (ty + 1) * TL::W + 2 + 2 * tx;  // even: 8-byte aligned
+  const int yc = min(yg, ny - 1);
+  const int own_g0 = yc * nx + min(xg, nx - 1);
+  const int own_g1 = yc * nx + min(xg + 1, nx - 1);
+  const bool has_halo = tid < TL::HALO;
+  int lx, ly;
+  if (tid < BX + 2) {
+    lx = 1 + tid;
+    ly = 0;
+  } else if (tid < 2 * (BX + 2)) {
+    lx = 1 + tid - (BX + 2);
+    ly = TL::H - 1;
+  } else if (tid < 2 * (BX + 2) + BY) {
+    lx = 1;
+    ly = 1 + tid - 2 * (BX + 2);
+  } else {
+    lx = BX + 2;
+    ly = 1 + tid - 2 * (BX + 2) - BY;
+  }
+  const int halo_s = ly * TL::W + lx;
+  const int halo_g = min(max(y0 - 1 + ly, 0), ny - 1) * nx +
+                     min(max(x0 - 2 + lx, 0), nx - 1);
+  const bool store0 = xg < nx && yg < ny;
+  const bool store1 = xg + 1 < nx && yg < ny;
+  const size_t plane = (size_t)nx * ny;
+  const Coef2 kk = coef2(k);
+
+  const int plim = min(z1, nz - 1);
+  int pn = z0;
+  const float* pbase = src + (size_t)z0 * plane;
+  auto load_next = [&]() -> MarchQuad {
+    MarchQuad v;
+    v.o0 = __ldg(pbase + own_g0);
+    v.o1 = __ldg(pbase + own_g1);
+    v.halo = has_halo ? __ldg(pbase + halo_g) : 0.0f;
+    if (pn < plim) pbase += plane;
+    ++pn;
+    return v;
+  };
+
+  MarchQuad q[kMarchQ];
+#pragma unroll
+  for (int i = 0; i < kMarchQ; ++i) q[i] = load_next();
+  float b0, b1;
+  if (z0 > 0) {
+    b0 = __ldg(src + (size_t)(z0 - 1) * plane + own_g0);
+    b1 = __ldg(src + (size_t)(z0 - 1) * plane + own_g1);
+  } else {
+    b0 = q[0].o0;
+    b1 = q[0].o1;
+  }
+  float* out = dst + (size_t)z0 * plane + own_g0;
+
+  auto plane_step = [&](float* st, MarchQuad& cur, const MarchQuad& next) {
+    *reinterpret_cast<float2*>(st + own_s) = make_float2(cur.o0, cur.o1);
+    if (has_halo) st[halo_s] = cur.halo;
+    const float c0 = cur.o0, c1 = cur.o1;
+    const uint64_t t01 = pack2(next.o0, next.o1);
+    const uint64_t b01 = pack2(b0, b1);
+    cur = load_next();
+    __syncthreads();
+    const float w0 = st[own_s - 1];
+    const float e1 = st[own_s + 2];
+    const float2 n = *reinterpret_cast<const float2*>(st + own_s - TL::W);
+    const float2 sv = *reinterpret_cast<const float2*>(st + own_s + TL::W);
+    const uint64_t r = point2(kk, pack2(c0, c1), pack2(w0, c0),
+                              pack2(c1, e1), pack2(sv.x, sv.y),
+                              pack2(n.x, n.y), b01, t01);
+    float o0, o1;
+    unpack2(r, o0, o1);
+    if (store0) out[0] = o0;
+    if (store1) out[1] = o1;
+    out += plane;
+    b0 = c0;
+    b1 = c1;
+  };
+
+  for (int z = z0; z < z1; z += kMarchQ) {
+    bool more = true;
+#pragma unroll
+    for (int i = 0; i < kMarchQ; ++i) {
+      if (more) {
+        plane_step(stage[i & 1], q[i], q[(i + 1) % kMarchQ]);
+        more = (z + i + 1 < z1);
+      }
+    }
+    if (!more) break;
+  }
+}
+
 }  // namespace d3d

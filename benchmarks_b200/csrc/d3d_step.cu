@@ -217,19 +217,43 @@ drain:
 // Generic kernel: any nx, ny, nz, any alignment -- d3d::march_tile over a
 // 32 x 8 tile and a z-chunk (d3d_march.cuh).
 // ---------------------------------------------------------------------------
-constexpr int kGenBX = 32;
-constexpr int kGenBY = 8;
+// FP32: two cells per thread on 64 x 8 tiles (packed arithmetic);
+// FP64: one cell per thread on 32 x 8 tiles.
+template <typename T> struct GenTile;
+template <> struct GenTile<float> { static constexpr int BX = 64, BY = 8; };
+template <> struct GenTile<double> { static constexpr int BX = 32, BY = 8; };
 
 template <typename T>
 __global__ void __launch_bounds__(256)
     step_generic_kernel(const T* __restrict__ src, T* __restrict__ dst,
-                        int nx, int ny, int nz, Coef<T> k, int zchunk) {
-  __shared__ T stage[2][MarchTile<kGenBX, kGenBY>::E];
+                        int nx, int ny, int nz, Coef<T> k, int zchunk);
+
+template <>
+__global__ void __launch_bounds__(256)
+    step_generic_kernel<float>(const float* __restrict__ src,
+                               float* __restrict__ dst, int nx, int ny,
+                               int nz, Coef<float> k, int zchunk) {
+  constexpr int BX = GenTile<float>::BX, BY = GenTile<float>::BY;
+  __shared__ __align__(16) float stage[2][MarchTile2<BX, BY>::E];
   const int z0 = blockIdx.z * zchunk;
   const int z1 = min(nz, z0 + zchunk);
   if (z0 >= z1) return;
-  march_tile<T, kGenBX, kGenBY>(src, dst, nx, ny, nz, blockIdx.x * kGenBX,
-                                blockIdx.y * kGenBY, z0, z1, k, stage);
+  march_tile2<BX, BY>(src, dst, nx, ny, nz, blockIdx.x * BX, blockIdx.y * BY,
+                      z0, z1, k, stage);
+}
+
+template <>
+__global__ void __launch_bounds__(256)
+    step_generic_kernel<double>(const double* __restrict__ src,
+                                double* __restrict__ dst, int nx, int ny,
+                                int nz, Coef<double> k, int zchunk) {
+  constexpr int BX = GenTile<double>::BX, BY = GenTile<double>::BY;
+  __shared__ double stage[2][MarchTile<BX, BY>::E];
+  const int z0 = blockIdx.z * zchunk;
+  const int z1 = min(nz, z0 + zchunk);
+  if (z0 >= z1) return;
+  march_tile<double, BX, BY>(src, dst, nx, ny, nz, blockIdx.x * BX,
+                             blockIdx.y * BY, z0, z1, k, stage);
 }
 
 // ---------------------------------------------------------------------------
@@ -382,12 +406,14 @@ cudaError_t launch_step_tma(const CUtensorMap& src, void* f2, int nx, int ny,
 cudaError_t launch_step_generic(const void* f1, void* f2, int nx, int ny,
                                 int nz, const void* coef, int dtype,
                                 cudaStream_t stream, LaunchInfo* info) {
-  const int gx = (nx + kGenBX - 1) / kGenBX;
-  const int gy = (ny + kGenBY - 1) / kGenBY;
+  const int bx = dtype == kF64 ? GenTile<double>::BX : GenTile<float>::BX;
+  const int by = dtype == kF64 ? GenTile<double>::BY : GenTile<float>::BY;
+  const int gx = (nx + bx - 1) / bx;
+  const int gy = (ny + by - 1) / by;
   const int zchunk = pick_zchunk(nz, (long)gx * gy, 8, 32);
   const int gz = (nz + zchunk - 1) / zchunk;
-  if (info) *info = LaunchInfo{gx, gy, gz, kGenBX * kGenBY, 0, zchunk, 8};
-  dim3 grid(gx, gy, gz), block(kGenBX * kGenBY);
+  if (info) *info = LaunchInfo{gx, gy, gz, 256, 0, zchunk, 8};
+  dim3 grid(gx, gy, gz), block(256);
   if (dtype == kF64)
     step_generic_kernel<double><<<grid, block, 0, stream>>>(
         static_cast<const double*>(f1), static_cast<double*>(f2), nx, ny, nz,
@@ -398,5 +424,6 @@ cudaError_t launch_step_generic(const void* f1, void* f2, int nx, int ny,
         coef_from<float>(coef), zchunk);
   return cudaGetLastError();
 }
+
 
 }  // namespace d3d
