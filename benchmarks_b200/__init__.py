@@ -78,6 +78,9 @@ _SIGNATURES = {
     "d3d_server_stats": ([_vp, ctypes.c_char_p, _sz], _i),
     "d3d_server_destroy": ([_vp], _i),
     "d3d_check_device_errors": ([ctypes.POINTER(ctypes.c_uint)], _i),
+    "d3d_accuracy": ([_vp, _vp, _i, _dp, _vp], _i),
+    "d3d_selftest_wait_timeout": ([ctypes.c_uint,
+                                   ctypes.POINTER(ctypes.c_uint)], _i),
 }
 
 _lib = None
@@ -281,6 +284,16 @@ class Plan:
         self._check_buf(out)
         check(lib().d3d_analytic(self._h, out.data_ptr(), float(time),
                                  _stream_handle(stream)))
+
+    def accuracy(self, field, count, stream=None):
+        """FP64 (rms, max_abs, max_rel, sum) of `field` against the analytic
+        solution after `count` steps, on the device."""
+        self._check_buf(field)
+        out = np.zeros(4, np.float64)
+        check(lib().d3d_accuracy(self._h, field.data_ptr(), count,
+                                 out.ctypes.data_as(_dp),
+                                 _stream_handle(stream)))
+        return out
 
     def compare(self, a, b, stream=None):
         """FP64 (rms, max_abs, max_rel, sum(a)) of device field a vs b."""

@@ -636,6 +636,51 @@ int d3d_compare_noalloc(const void* a, int a_dtype, const void* b,
   return D3D_OK;
 }
 
+int d3d_accuracy(d3d_plan p, const void* field, int count, double out[4],
+                 void* stream) {
+  if (!p || !field || !out) return fail(D3D_E_INVALID, "NULL argument");
+  if (count < 0) return fail(D3D_E_INVALID, "negative count %d", count);
+  int rc = check_device(p);
+  if (rc) return rc;
+  cudaStream_t s = as_stream(stream);
+  if (!p->cmp_scratch)
+    D3D_TRY(cudaMalloc(&p->cmp_scratch, d3d::compare_scratch_bytes()),
+            "cudaMalloc (compare scratch)");
+  // time = count * dt in the plan's precision, as GetCorrectAnswer forms it
+  // (diffusion3d.h:113-120); the closed form itself in double.
+  double time;
+  if (p->dtype == kF64) {
+    double g[8];
+    reference_coefficients<double>(p->nx, p->ny, p->nz, nullptr, g);
+    time = (double)count * g[7];
+  } else {
+    float g[8];
+    reference_coefficients<float>(p->nx, p->ny, p->nz, nullptr, g);
+    time = (double)((float)count * g[7]);
+  }
+  double g64[8];
+  reference_coefficients<double>(p->nx, p->ny, p->nz, nullptr, g64);
+  D3D_TRY(d3d::launch_accuracy(field, p->dtype, p->nx, p->ny, p->nz, g64[4],
+                               g64[5], g64[6], g64[1], g64[2], g64[3], g64[0],
+                               time, p->cmp_scratch, s),
+          "accuracy launch");
+  g_launches.fetch_add(2, std::memory_order_relaxed);
+  D3D_TRY(cudaMemcpyAsync(out, p->cmp_scratch, 4 * sizeof(double),
+                          cudaMemcpyDeviceToHost, s),
+          "D2H copy");
+  D3D_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  return D3D_OK;
+}
+
+int d3d_selftest_wait_timeout(unsigned iterations, unsigned* flags_out) {
+  unsigned* err = dev_error_ptr();
+  if (!err) return fail(D3D_E_CUDA, "cannot resolve device error word");
+  D3D_TRY(d3d::launch_selftest_wait(iterations, err, nullptr),
+          "self-test launch");
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return d3d_check_device_errors(flags_out);
+}
+
 int d3d_check_device_errors(unsigned* flags_out) {
   D3D_TRY(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
   unsigned* p = dev_error_ptr();

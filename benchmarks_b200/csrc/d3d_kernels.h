@@ -104,6 +104,17 @@ cudaError_t launch_batch_step(int shape, const BatchDesc* descs,
                               const int2* items, int nitems, int parity,
                               cudaStream_t s);
 
+// FP64 error norms of a field against the analytic solution at `time`,
+// evaluated per point (no analytic buffer); result in scratch[0..3].
+cudaError_t launch_accuracy(const void* f, int dtype, int nx, int ny, int nz,
+                            double kx, double ky, double kz, double dx,
+                            double dy, double dz, double kappa, double time,
+                            double* scratch, cudaStream_t stream);
+
+// A one-CTA kernel whose bounded mbarrier wait is bound to run out.
+cudaError_t launch_selftest_wait(unsigned limit, unsigned* dev_err,
+                                 cudaStream_t stream);
+
 // Analytic solution (the reference's Initialize, computed in FP64 on the
 // device) written in `dtype` at `time`.
 cudaError_t launch_analytic(void* out, int dtype, int nx, int ny, int nz,

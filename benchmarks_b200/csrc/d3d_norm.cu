@@ -121,6 +121,59 @@ __global__ void analytic_kernel(T* out, int nx, int ny, int nz, double kx,
   }
 }
 
+// Field against the analytic solution, the analytic value evaluated per
+// point in double (no analytic buffer): one read of the field.
+template <typename T>
+__global__ void __launch_bounds__(kCmpThreads)
+    accuracy_partial_kernel(const T* f, int nx, int ny, int nz, double kx,
+                            double ky, double kz, double dx, double dy,
+                            double dz, double ax, double ay, double az,
+                            double* partial) {
+  Acc v = {0, 0, 0, 0};
+  const size_t n = (size_t)nx * ny * nz;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += stride) {
+    const int jx = (int)(i % nx);
+    const int jy = (int)((i / nx) % ny);
+    const int jz = (int)(i / ((size_t)nx * ny));
+    const double y_ref = 0.125 * (1.0 - ax * cos(kx * (dx * (jx + 0.5)))) *
+                         (1.0 - ay * cos(ky * (dy * (jy + 0.5)))) *
+                         (1.0 - az * cos(kz * (dz * (jz + 0.5))));
+    const double x = (double)f[i];
+    const double d = x - y_ref;
+    const double ad = fabs(d);
+    v.ss += d * d;
+    v.mx = fmax(v.mx, ad);
+    v.mr = fmax(v.mr, ad / fmax(fabs(y_ref), 1e-300));
+    v.sa += x;
+  }
+  Acc r = block_reduce(v);
+  if (threadIdx.x == 0) {
+    double* p = partial + 4 * (size_t)blockIdx.x;
+    p[0] = r.ss;
+    p[1] = r.mx;
+    p[2] = r.mr;
+    p[3] = r.sa;
+  }
+}
+
+// One CTA waits, with a short bound, on an mbarrier phase that nothing
+// completes (no thread ever arrives): the bounded-wait failure path every
+// TMA kernel relies on, exercised without a fault.
+__global__ void selftest_wait_kernel(unsigned limit, unsigned* dev_err) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  bool done = false;
+  for (unsigned i = 0; i < limit && !done; ++i) done = mbar_try_wait(&bar, 0);
+  if (!__syncthreads_or(done) && threadIdx.x == 0)
+    atomicOr(dev_err, kDevWaitTimeout);
+}
+
 template <typename TA>
 cudaError_t launch_partial(const void* a, const void* b, int b_dtype, size_t n,
                            double* partial, int blocks, cudaStream_t s) {
@@ -256,6 +309,35 @@ cudaError_t launch_compare(const void* a, int a_dtype, const void* b,
   if (e != cudaSuccess) return e;
   compare_final_kernel<<<1, kCmpThreads, 0, stream>>>(partial, blocks, n,
                                                       scratch);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_accuracy(const void* f, int dtype, int nx, int ny, int nz,
+                            double kx, double ky, double kz, double dx,
+                            double dy, double dz, double kappa, double time,
+                            double* scratch, cudaStream_t stream) {
+  const double ax = exp(-kappa * time * (kx * kx));
+  const double ay = exp(-kappa * time * (ky * ky));
+  const double az = exp(-kappa * time * (kz * kz));
+  double* partial = scratch + 4;
+  if (dtype == kF64)
+    accuracy_partial_kernel<double><<<kCmpBlocks, kCmpThreads, 0, stream>>>(
+        static_cast<const double*>(f), nx, ny, nz, kx, ky, kz, dx, dy, dz, ax,
+        ay, az, partial);
+  else
+    accuracy_partial_kernel<float><<<kCmpBlocks, kCmpThreads, 0, stream>>>(
+        static_cast<const float*>(f), nx, ny, nz, kx, ky, kz, dx, dy, dz, ax,
+        ay, az, partial);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  compare_final_kernel<<<1, kCmpThreads, 0, stream>>>(
+      partial, kCmpBlocks, (size_t)nx * ny * nz, scratch);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_selftest_wait(unsigned limit, unsigned* dev_err,
+                                 cudaStream_t stream) {
+  selftest_wait_kernel<<<1, 32, 0, stream>>>(limit, dev_err);
   return cudaGetLastError();
 }
 

@@ -272,6 +272,22 @@ int d3d_server_destroy(d3d_server server);
 int d3d_compare_noalloc(const void* a, int a_dtype, const void* b,
                         int b_dtype, size_t n, double out[4], void* stream);
 
+/* The reference's accuracy report computed on the device: the field (plan
+ * shape and dtype) against the analytic solution after `count` steps
+ * (GetCorrectAnswer, diffusion3d.h:113-120; GetAccuracy, baseline.cc:51-60),
+ * with the closed form evaluated per point in double and the errors summed in
+ * double -- one read of the field, no analytic buffer.  out = rms, max_abs,
+ * max_rel, sum(field).  (The reference sums in float sequentially on the
+ * host; its figure is reproduced there, this is the FP64 report.) */
+int d3d_accuracy(d3d_plan plan, const void* field, int count, double out[4],
+                 void* stream);
+
+/* Failure-path self-test: launches one CTA whose mbarrier wait (bounded by
+ * `iterations` tries) can never complete, and returns what
+ * d3d_check_device_errors returns afterwards -- D3D_E_TIMEOUT with the
+ * timeout flag set, and a context that stays usable.  No fault, no trap. */
+int d3d_selftest_wait_timeout(unsigned iterations, unsigned* flags_out);
+
 /* Reads and clears the device error word that kernels set instead of
  * trapping when a bounded wait runs out; returns D3D_E_TIMEOUT if any bit
  * was set.  Synchronises the current device. */

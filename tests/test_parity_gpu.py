@@ -331,3 +331,36 @@ def test_maximum_sizes(dims):
     got = np.array([outs[0][z, y, x].item() for z, y, x in idx], np.float32)
     assert got.tobytes() == ref.tobytes()
     assert B.check_device_errors() == 0
+
+
+def test_device_accuracy_matches_oracle_fp64_report():
+    """d3d_accuracy (analytic form evaluated per point in double, errors
+    summed in double) against the oracle's FP64 analytic field and norms;
+    the reference's float GetAccuracy agrees to float rounding."""
+    nx, ny, nz, count = 48, 40, 36, 23
+    c, g = O.params(nx, ny, nz)
+    fin = O.initialize(nx, ny, nz)
+    ref = O.run(fin, c, count)
+    plan = B.Plan(nx, ny, nz)
+    got = plan.accuracy(torch.from_numpy(ref).cuda(), count)
+    t = float(np.float32(count) * g[7])
+    ana = O.initialize(nx, ny, nz, time=t, dtype=np.float64)
+    exp = O.norms(ref, ana)
+    np.testing.assert_allclose(got[[0, 3]], exp[[0, 3]], rtol=1e-9)
+    np.testing.assert_allclose(got[1], exp[1], rtol=1e-9)
+    # the reference's figure: float analytic field, float running sum
+    assert got[0] == pytest.approx(O.accuracy(ref, count), rel=1e-3)
+
+
+def test_bounded_wait_timeout_leaves_context_usable():
+    """The failure path of every bounded mbarrier wait: a wait that can
+    never complete runs out, sets the device error word, and the next
+    kernels run normally."""
+    flags = B.ctypes.c_uint()
+    rc = B.lib().d3d_selftest_wait_timeout(2000, B.ctypes.byref(flags))
+    assert rc == B.D3D_E_TIMEOUT and flags.value & 1
+    assert B.check_device_errors() == 0  # read-and-clear
+    nx, ny, nz = 64, 16, 9
+    c, _ = O.params(nx, ny, nz)
+    fin = O.seeded_noise((nz, ny, nx), 1, amplitude=1.0)
+    assert bits_equal(gpu_run(fin, c, 3), O.run(fin, c, 3))

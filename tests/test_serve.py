@@ -91,3 +91,18 @@ def test_zero_step_requests_return_their_input():
              O.params(7, 6, 5)[0])]
     outs, _ = _serve(reqs)
     assert outs[0].tobytes() == reqs[0][0].tobytes()
+
+
+def test_arena_allocation_failure_is_reported():
+    """Host-visible failure: an arena larger than the device fails cleanly
+    with D3D_E_OOM and leaves the process usable."""
+    with pytest.raises(B.D3DError) as ei:
+        B.Server(1 << 50)
+    assert ei.value.code == B.D3D_E_OOM
+    server = B.Server(1 << 24)
+    f = O.seeded_noise((8, 8, 8), 1, amplitude=1.0)
+    o = np.zeros_like(f)
+    server.submit(f, o, 2, O.params(8, 8, 8)[0])
+    server.drain()
+    assert o.tobytes() == O.run(f, O.params(8, 8, 8)[0], 2).tobytes()
+    server.close()
