@@ -354,7 +354,6 @@ def run_b200(args):
     stream = torch.cuda.current_stream()
     plan = B.Plan(n, n, n, B.F32, B.KERNEL_AUTO)
     coeff = plan.reference_coefficients()
-    _, geom = B.coefficients(n, n, n, B.F32)
 
     # Config: analytic sinusoid at t=0 plus seeded U[0, 1e-3) noise.
     f1 = plan.empty()
@@ -448,22 +447,27 @@ def run_b200(args):
     x2 = torch.empty_like(x1)
     r32, o32 = plan.run(x1, x2, COUNT, coeff, stream)
     del o32
-    ana = torch.empty_like(r64)
-    t_final = float(np.float32(COUNT) * geom[7])  # count * dt_, as the reference
-    plan64.analytic(ana, t_final, stream)
-    def norms(v):
-        return {"rms": v[0], "max_abs": v[1], "max_rel": v[2]}
+
+    def norms(v, rel=True):
+        d = {"rms": v[0], "max_abs": v[1]}
+        if rel:
+            d["max_rel"] = v[2]
+        return d
+    # Errors against the analytic decay: the closed form is evaluated per
+    # point in FP64 on the device (d3d_accuracy); the input's noise is part
+    # of that error, so only rms / max_abs are meaningful there.
     report = {
         "fp32_vs_fp64": norms(plan.compare(r32, r64, stream)),
-        "fp32_vs_analytic": norms(plan.compare(r32, ana, stream)),
-        "fp64_vs_analytic": norms(plan.compare(r64, ana, stream)),
+        "fp32_vs_analytic": norms(plan.accuracy(r32, COUNT, stream), False),
+        "fp64_vs_analytic": norms(plan64.accuracy(r64, COUNT, stream), False),
         "steps": COUNT, "input": "analytic(t=0) + U[0,1e-3) noise",
+        "tolerance": "max_rel(fp32 vs fp64) <= 1e-5",
     }
     # FP64 throughput of the same workload (16 B per update).
     r64_rate, _ = rate_of(plan64, g1, g2, 2)
     side["fp64"] = {"value": r64_rate, "unit": UNIT,
                     "hbm_frac": r64_rate * 16 / peak}
-    del g1, g2, r64, ana, x1, x2, r32, init
+    del g1, g2, r64, x1, x2, r32, init
     plan64.close()
     torch.cuda.synchronize()
 
