@@ -151,8 +151,10 @@ int d3d_compare(d3d_plan plan, const void* a, int a_dtype, const void* b,
 
 /* ---------------------------------------------------------------------
  * Batched solves: many independent FP32 grids of different shapes,
- * coefficients and step counts advanced by ONE persistent multi-grid
- * kernel.  No counterpart in the reference (which runs one grid per
+ * coefficients and step counts advanced together -- one multi-grid step
+ * kernel per size class and time step, the whole run captured once into a
+ * CUDA graph and replayed as one graph launch.  No counterpart in the
+ * reference (which runs one grid per
  * process); each grid's arithmetic is still RunKernel's, so every grid's
  * result is bit-identical to running it alone (with the reference or with
  * d3d_run).

@@ -11,6 +11,14 @@
  *   d3do_step_{f32,f64}        Diffusion3DOpenMP::RunKernel   diffusion3d_openmp.cc:43-71
  *   d3do_run_{f32,f64}         (same, `count` steps)
  *   d3do_accuracy_{f32,f64}    Baseline::GetAccuracy          baseline.cc:51-60
+ * and of the second plugin surface, diffusion::Diffusion (src/diffusion;
+ * bodies in dif_oracle_impl.h):
+ *   difo_params_{f32,f64}      Diffusion::Diffusion           diffusion.h:93-108
+ *   difo_initialize_{f32,f64}  Initialize                     diffusion.h:48-77
+ *                              DiffusionOpenMP::Initialize2D/3D diffusion_openmp.cc:5-49
+ *   difo_step_{f32,f64}        DiffusionOpenMP::RunKernel2D/3D diffusion_openmp.cc:59-112
+ *   difo_run_{f32,f64}         (same, `count` steps)
+ *   difo_accuracy_{f32,f64}    Baseline::GetAccuracy          baseline.h:86-95
  * plus FP64-accumulated error norms between two fields (no reference
  * counterpart: the FP64 error report the reference lacks).
  *
@@ -37,6 +45,7 @@
 #define COS_R cosf
 #define SQRT_R sqrtf
 #include "d3d_oracle_impl.h"
+#include "dif_oracle_impl.h"
 #undef REAL
 #undef SFX
 #undef EXP_R
@@ -50,6 +59,7 @@
 #define COS_R cos
 #define SQRT_R sqrt
 #include "d3d_oracle_impl.h"
+#include "dif_oracle_impl.h"
 #undef REAL
 #undef SFX
 #undef EXP_R

@@ -51,3 +51,12 @@ def oracle_mod():
     import oracle
     oracle.lib()
     return oracle
+
+
+@pytest.fixture(scope="session")
+def golden_diffusion():
+    """Fixtures of the diffusion::Diffusion surface (2D and 3D grids)."""
+    with open(os.path.join(GOLDEN_DIR, "diffusion.json")) as f:
+        meta = json.load(f)
+    fields = np.load(os.path.join(GOLDEN_DIR, "diffusion_fields.npz"))
+    return meta, fields
