@@ -40,6 +40,10 @@ _SIGNATURES = {
     "d3d_launch_count": ([], ctypes.c_ulonglong),
     "d3d_coefficients": ([_i, _i, _i, _i, _vp, _vp], _i),
     "d3d_plan_create": ([_i, _i, _i, _i, _i, _i, _vpp], _i),
+    "d3d_diffusion_coefficients": ([_i, ctypes.POINTER(ctypes.c_int), _i,
+                                    _vp, _vp], _i),
+    "d3d_diffusion_plan_create": ([_i, ctypes.POINTER(ctypes.c_int), _i, _i,
+                                   _i, _vpp], _i),
     "d3d_plan_set_tile": ([_vp, _i, _i], _i),
     "d3d_plan_set_graphs": ([_vp, _i], _i),
     "d3d_plan_autotune": ([_vp, _vp, _vp, _vp, _i, _vp, _dp], _i),
@@ -163,6 +167,8 @@ def _torch_dtype(dtype):
 class Plan:
     """A d3d_plan: one grid shape, precision and kernel choice."""
 
+    ndim = 3
+
     def __init__(self, nx, ny, nz, dtype=F32, kernel=KERNEL_AUTO, tb_depth=1,
                  variant=None, zchunk=0):
         self.nx, self.ny, self.nz = nx, ny, nz
@@ -170,11 +176,14 @@ class Plan:
         self.kernel = kernel
         self.tb_depth = tb_depth
         h = ctypes.c_void_p()
-        check(lib().d3d_plan_create(nx, ny, nz, dtype, kernel, tb_depth,
-                                    ctypes.byref(h)))
+        check(self._create(ctypes.byref(h)))
         self._h = h
         if variant is not None or zchunk:
             self.set_tile(variant or 0, zchunk)
+
+    def _create(self, out):
+        return lib().d3d_plan_create(self.nx, self.ny, self.nz, self.dtype,
+                                     self.kernel, self.tb_depth, out)
 
     @property
     def handle(self):
@@ -236,10 +245,17 @@ class Plan:
         return c
 
     # --- compute entry points (device buffers: torch tensors) -----------
+    @property
+    def shape(self):
+        """Array shape of one field: (nz, ny, nx), or (ny, nx) in 2D."""
+        if self.ndim == 2:
+            return (self.ny, self.nx)
+        return (self.nz, self.ny, self.nx)
+
     def empty(self):
         import torch
-        return torch.empty((self.nz, self.ny, self.nx),
-                           dtype=_torch_dtype(self.dtype), device="cuda")
+        return torch.empty(self.shape, dtype=_torch_dtype(self.dtype),
+                           device="cuda")
 
     def _check_buf(self, t):
         assert t.is_cuda and t.is_contiguous() and t.numel() == self.n
@@ -306,6 +322,43 @@ class Plan:
                                 out.ctypes.data_as(_dp),
                                 _stream_handle(stream)))
         return out
+
+
+def diffusion_coefficients(nd, dims, dtype=F32):
+    """(coeff[7], geom[8]) as diffusion::Diffusion(nd, dims) derives them
+    (dims = (nx, ny) or (nx, ny, nz))."""
+    c = np.zeros(7, np_dtype(dtype))
+    g = np.zeros(8, np_dtype(dtype))
+    d = (ctypes.c_int * len(dims))(*dims)
+    check(lib().d3d_diffusion_coefficients(nd, d, dtype, c.ctypes.data,
+                                           g.ctypes.data))
+    return c, g
+
+
+class DiffusionPlan(Plan):
+    """A plan for the reference's diffusion::Diffusion surface: a 2D
+    5-point grid (dims = (nx, ny)) or a 3D grid (dims = (nx, ny, nz)) summed
+    in that surface's order.  Fields are (ny, nx) or (nz, ny, nx) arrays."""
+
+    def __init__(self, dims, dtype=F32, kernel=KERNEL_AUTO, tb_depth=1,
+                 variant=None, zchunk=0):
+        dims = tuple(int(d) for d in dims)
+        if len(dims) not in (2, 3):
+            raise ValueError("dims must be (nx, ny) or (nx, ny, nz)")
+        self.ndim = len(dims)
+        self.dims = dims
+        nz = dims[2] if self.ndim == 3 else 1
+        super().__init__(dims[0], dims[1], nz, dtype, kernel, tb_depth,
+                         variant, zchunk)
+
+    def _create(self, out):
+        d = (ctypes.c_int * self.ndim)(*self.dims)
+        return lib().d3d_diffusion_plan_create(self.ndim, d, self.dtype,
+                                               self.kernel, self.tb_depth,
+                                               out)
+
+    def reference_coefficients(self):
+        return diffusion_coefficients(self.ndim, self.dims, self.dtype)[0]
 
 
 class BatchGrid(ctypes.Structure):

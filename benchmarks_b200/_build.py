@@ -37,9 +37,9 @@ NVCC_FLAGS = ARCH + [
     "-I" + INCLUDE, "-I" + CSRC,
 ]
 
-SOURCES = ["d3d_step.cu", "d3d_tb.cu", "d3d_norm.cu", "d3d_batch.cu",
-           "d3d_serve.cu", "d3d_api.cu"]
-HEADERS = ["d3d_common.cuh", "d3d_kernels.h"]
+SOURCES = ["d3d_step.cu", "d3d_step2d.cu", "d3d_tb.cu", "d3d_norm.cu",
+           "d3d_batch.cu", "d3d_serve.cu", "d3d_api.cu"]
+HEADERS = ["d3d_common.cuh", "d3d_kernels.h", "d3d_march.cuh"]
 
 
 def _mtime(p):

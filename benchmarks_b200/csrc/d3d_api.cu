@@ -20,6 +20,10 @@
 using d3d::kF32;
 using d3d::kF64;
 
+static_assert(d3d::kNumTmaVariants == D3D_NUM_TILE_VARIANTS &&
+                  d3d::kNumStep2dVariants == D3D_NUM_TILE_VARIANTS,
+              "d3d_plan_set_tile takes one variant range for 2D and 3D");
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -99,6 +103,21 @@ void reference_coefficients(int nx, int ny, int nz, T* coeff, T* geom) {
   }
 }
 
+// diffusion::Diffusion::Diffusion(nd, dims) (diffusion.h:93-108): the
+// geometry and ce..cb of the diffusion3d constructor (ny = 1 below 2D,
+// nz = 1 below 3D), but cc adds the z pair as a unit, and only in 3D:
+// cc = 1.0 - (ce + cw + cn + cs + (nd == 3 ? ct + cb : 0)).
+template <typename T>
+void diffusion_coefficients(int nd, int nx, int ny, int nz, T* coeff,
+                            T* geom) {
+  T c[7];
+  reference_coefficients<T>(nx, ny, nz, c, geom);
+  const T xy = c[0] + c[1] + c[2] + c[3];
+  const T zpair = nd == 3 ? (T)(c[4] + c[5]) : (T)0;
+  c[6] = (T)(1.0 - (double)(xy + zpair));
+  if (coeff) memcpy(coeff, c, sizeof c);
+}
+
 }  // namespace
 
 namespace d3d {
@@ -121,6 +140,11 @@ void note_launches(unsigned long long n) {
 
 struct d3d_plan_s {
   int nx, ny, nz, dtype, kernel, tb_depth;
+  // 3 for 3D grids, 2 for the 2D grids of the diffusion::Diffusion surface.
+  int ndim;
+  // Sum the y-1 neighbour before y+1 (diffusion::Diffusion) instead of
+  // after it (diffusion3d).
+  int flip_y;
   int variant;  // TMA tile variant
   int zchunk;   // 0 = automatic
   int device;
@@ -189,6 +213,14 @@ int check_device(d3d_plan p) {
 // One single-step launch, choosing the TMA path when the buffer allows it.
 int step_once(d3d_plan p, const void* f1, void* f2, const void* coeff,
               cudaStream_t s) {
+  if (p->ndim == 2) {
+    D3D_TRY(d3d::launch_step2d(f1, f2, p->nx, p->ny, coeff, p->dtype,
+                               p->variant, p->zchunk, s, &p->last),
+            "step2d launch");
+    p->last_kernel = "step2d";
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return D3D_OK;
+  }
   const bool use_tma = p->kernel != D3D_KERNEL_GENERIC &&
                        d3d::tma_eligible(f1, p->nx, p->ny, p->dtype);
   if (p->kernel == D3D_KERNEL_TMA && !use_tma)
@@ -201,13 +233,13 @@ int step_once(d3d_plan p, const void* f1, void* f2, const void* coeff,
                      d3d::tma_box_y(p->variant), &map);
     if (rc) return rc;
     D3D_TRY(d3d::launch_step_tma(*map, f2, p->nx, p->ny, p->nz, coeff,
-                                 p->dtype, p->variant, p->zchunk, s,
-                                 dev_error_ptr(), &p->last),
+                                 p->dtype, p->variant, p->zchunk, p->flip_y,
+                                 s, dev_error_ptr(), &p->last),
             "step_tma launch");
     p->last_kernel = "step_tma";
   } else {
     D3D_TRY(d3d::launch_step_generic(f1, f2, p->nx, p->ny, p->nz, coeff,
-                                     p->dtype, s, &p->last),
+                                     p->dtype, p->flip_y, s, &p->last),
             "step_generic launch");
     p->last_kernel = "step_generic";
   }
@@ -223,8 +255,8 @@ int tb_pass(d3d_plan p, const void* f1, void* f2, const void* coeff,
                    &map);
   if (rc) return rc;
   D3D_TRY(d3d::launch_steps_tb(*map, f2, p->nx, p->ny, p->nz, coeff, p->dtype,
-                               p->tb_depth, p->zchunk, s, dev_error_ptr(),
-                               &p->last),
+                               p->tb_depth, p->zchunk, p->flip_y, s,
+                               dev_error_ptr(), &p->last),
           "temporal-blocking launch");
   p->last_kernel = "steps_tb";
   g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -353,8 +385,12 @@ int d3d_coefficients(int nx, int ny, int nz, int dtype, void* coeff7,
   return D3D_OK;
 }
 
-int d3d_plan_create(int nx, int ny, int nz, int dtype, int kernel,
-                    int tb_depth, d3d_plan* out) {
+}  // extern "C"
+
+namespace {
+
+int plan_new(int ndim, int flip_y, int nx, int ny, int nz, int dtype,
+             int kernel, int tb_depth, d3d_plan* out) {
   if (!out) return fail(D3D_E_INVALID, "out is NULL");
   *out = nullptr;
   if (!valid_dims(nx, ny, nz))
@@ -363,6 +399,10 @@ int d3d_plan_create(int nx, int ny, int nz, int dtype, int kernel,
     return fail(D3D_E_INVALID, "bad dtype %d", dtype);
   if (kernel < D3D_KERNEL_AUTO || kernel > D3D_KERNEL_TB)
     return fail(D3D_E_INVALID, "bad kernel %d", kernel);
+  if (ndim == 2 && (kernel == D3D_KERNEL_TMA || kernel == D3D_KERNEL_TB))
+    return fail(D3D_E_UNSUPPORTED,
+                "2D grids run the register-march kernel (AUTO or GENERIC); "
+                "the TMA and temporal-blocking kernels are 3D");
   if (kernel == D3D_KERNEL_TB && !d3d::tb_supported(tb_depth, dtype))
     return fail(D3D_E_UNSUPPORTED, "temporal blocking depth %d unsupported",
                 tb_depth);
@@ -373,10 +413,13 @@ int d3d_plan_create(int nx, int ny, int nz, int dtype, int kernel,
   p->nx = nx;
   p->ny = ny;
   p->nz = nz;
+  p->ndim = ndim;
+  p->flip_y = flip_y;
   p->dtype = dtype;
   p->kernel = kernel;
   p->tb_depth = kernel == D3D_KERNEL_TB ? tb_depth : 1;
-  p->variant = d3d::default_tma_variant(ny);
+  p->variant = ndim == 2 ? d3d::default_step2d_variant()
+                         : d3d::default_tma_variant(ny);
   p->zchunk = 0;
   p->device = dev;
   p->n = (size_t)nx * ny * nz;
@@ -391,6 +434,55 @@ int d3d_plan_create(int nx, int ny, int nz, int dtype, int kernel,
   }
   *out = p;
   return D3D_OK;
+}
+
+// nd and dims as diffusion::Diffusion takes them (main.cc builds dims as
+// nd copies of --size); 0 on success with nx, ny, nz filled.
+int diffusion_dims(int nd, const int* dims, int* nx, int* ny, int* nz) {
+  if (!dims) return fail(D3D_E_INVALID, "dims is NULL");
+  if (nd != 2 && nd != 3)
+    return fail(D3D_E_INVALID, "nd must be 2 or 3, got %d", nd);
+  *nx = dims[0];
+  *ny = dims[1];
+  *nz = nd == 3 ? dims[2] : 1;
+  if (!valid_dims(*nx, *ny, *nz))
+    return fail(D3D_E_INVALID, "bad dims %dx%dx%d", *nx, *ny, *nz);
+  return D3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int d3d_plan_create(int nx, int ny, int nz, int dtype, int kernel,
+                    int tb_depth, d3d_plan* out) {
+  return plan_new(3, 0, nx, ny, nz, dtype, kernel, tb_depth, out);
+}
+
+int d3d_diffusion_coefficients(int nd, const int* dims, int dtype,
+                               void* coeff7, void* geom8) {
+  int nx = 0, ny = 0, nz = 0;
+  int rc = diffusion_dims(nd, dims, &nx, &ny, &nz);
+  if (rc) return rc;
+  if (dtype == kF64)
+    diffusion_coefficients<double>(nd, nx, ny, nz,
+                                   static_cast<double*>(coeff7),
+                                   static_cast<double*>(geom8));
+  else if (dtype == kF32)
+    diffusion_coefficients<float>(nd, nx, ny, nz, static_cast<float*>(coeff7),
+                                  static_cast<float*>(geom8));
+  else
+    return fail(D3D_E_INVALID, "bad dtype %d", dtype);
+  return D3D_OK;
+}
+
+int d3d_diffusion_plan_create(int nd, const int* dims, int dtype, int kernel,
+                              int tb_depth, d3d_plan* out) {
+  if (out) *out = nullptr;
+  int nx = 0, ny = 0, nz = 0;
+  int rc = diffusion_dims(nd, dims, &nx, &ny, &nz);
+  if (rc) return rc;
+  return plan_new(nd, 1, nx, ny, nz, dtype, kernel, tb_depth, out);
 }
 
 int d3d_plan_set_tile(d3d_plan p, int variant, int zchunk) {
@@ -414,14 +506,21 @@ int d3d_plan_autotune(d3d_plan p, void* f1, void* f2, const void* coeff,
   cudaStream_t s = as_stream(stream);
   const bool tb = p->kernel == D3D_KERNEL_TB;
   if (tb) steps = std::max(steps / p->tb_depth, 1) * p->tb_depth;
-  const int zchunks[] = {0, 16, 32, 64, 128, 256};
-  const int nvariants = tb ? 1 : d3d::kNumTmaVariants;
+  const int zchunks3[] = {0, 16, 32, 64, 128, 256};
+  const int zchunks2[] = {0, 2, 4, 6, 8, 12, 16, 32};  // rows per warp task
+  const int* zchunks = p->ndim == 2 ? zchunks2 : zchunks3;
+  const int nzc = p->ndim == 2 ? 8 : 6;
+  const int nvariants = tb ? 1
+                        : p->ndim == 2 ? d3d::kNumStep2dVariants
+                                       : d3d::kNumTmaVariants;
+  const int zext = p->ndim == 2 ? p->ny : p->nz;  // marched extent
   const int old_variant = p->variant, old_zchunk = p->zchunk;
   float best = -1.0f;
   int best_v = old_variant, best_z = old_zchunk;
   for (int v = 0; v < nvariants; ++v) {
-    for (int zc : zchunks) {
-      if (zc != 0 && zc >= p->nz) continue;
+    for (int zi = 0; zi < nzc; ++zi) {
+      const int zc = zchunks[zi];
+      if (zc != 0 && zc >= zext) continue;
       if (!tb) p->variant = v;
       p->zchunk = zc;
       for (auto& m : p->maps) m.ptr = nullptr;
@@ -480,12 +579,15 @@ int d3d_plan_info(d3d_plan p, char* buf, size_t len) {
   if (!p || !buf) return fail(D3D_E_INVALID, "NULL argument");
   const auto& L = p->last;
   snprintf(buf, len,
-           "{\"nx\": %d, \"ny\": %d, \"nz\": %d, \"dtype\": \"%s\", "
+           "{\"nx\": %d, \"ny\": %d, \"nz\": %d, \"ndim\": %d, "
+           "\"surface\": \"%s\", \"dtype\": \"%s\", "
            "\"kernel\": %d, \"tb_depth\": %d, \"variant\": %d, "
            "\"zchunk\": %d, \"device\": %d, \"last_kernel\": \"%s\", "
            "\"grid\": [%d, %d, %d], \"block\": %d, \"smem\": %d, "
            "\"launch_zchunk\": %d, \"ctas_per_sm\": %d, \"graphs\": %d}",
-           p->nx, p->ny, p->nz, p->dtype == kF64 ? "f64" : "f32", p->kernel,
+           p->nx, p->ny, p->nz, p->ndim,
+           p->flip_y ? "diffusion" : "diffusion3d",
+           p->dtype == kF64 ? "f64" : "f32", p->kernel,
            p->tb_depth, p->variant, p->zchunk, p->device, p->last_kernel,
            L.grid_x, L.grid_y, L.grid_z, L.block, L.smem_bytes, L.zchunk,
            L.ctas_per_sm, p->use_graphs);
@@ -580,8 +682,8 @@ int d3d_analytic(d3d_plan p, void* out, double time, void* stream) {
   if (rc) return rc;
   double g[8];
   reference_coefficients<double>(p->nx, p->ny, p->nz, nullptr, g);
-  D3D_TRY(d3d::launch_analytic(out, p->dtype, p->nx, p->ny, p->nz, g[4], g[5],
-                               g[6], g[1], g[2], g[3], g[0], time,
+  D3D_TRY(d3d::launch_analytic(out, p->dtype, p->ndim, p->nx, p->ny, p->nz,
+                               g[4], g[5], g[6], g[1], g[2], g[3], g[0], time,
                                as_stream(stream)),
           "analytic launch");
   g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -660,9 +762,9 @@ int d3d_accuracy(d3d_plan p, const void* field, int count, double out[4],
   }
   double g64[8];
   reference_coefficients<double>(p->nx, p->ny, p->nz, nullptr, g64);
-  D3D_TRY(d3d::launch_accuracy(field, p->dtype, p->nx, p->ny, p->nz, g64[4],
-                               g64[5], g64[6], g64[1], g64[2], g64[3], g64[0],
-                               time, p->cmp_scratch, s),
+  D3D_TRY(d3d::launch_accuracy(field, p->dtype, p->ndim, p->nx, p->ny,
+                               p->nz, g64[4], g64[5], g64[6], g64[1], g64[2],
+                               g64[3], g64[0], time, p->cmp_scratch, s),
           "accuracy launch");
   g_launches.fetch_add(2, std::memory_order_relaxed);
   D3D_TRY(cudaMemcpyAsync(out, p->cmp_scratch, 4 * sizeof(double),

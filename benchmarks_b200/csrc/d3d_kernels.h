@@ -45,24 +45,47 @@ bool tma_eligible(const void* ptr, int nx, int ny, int dtype);
 cudaError_t encode_field_map(CUtensorMap* map, const void* ptr, int nx, int ny,
                              int nz, int dtype, int box_x, int box_y);
 
+// Every 3D launcher takes `flip_y`: 0 sums the y+1 neighbour 4th and y-1
+// 5th (diffusion3d, diffusion3d_openmp.cc:57-62); 1 sums y-1 4th and y+1
+// 5th (the diffusion::Diffusion surface, diffusion_openmp.cc:98-103).
+
 // One time step, f2 = stencil(f1), with the TMA-staged z-march.
 cudaError_t launch_step_tma(const CUtensorMap& src, void* f2, int nx, int ny,
                             int nz, const void* coef, int dtype, int variant,
-                            int zchunk_override, cudaStream_t stream,
-                            unsigned* dev_err, LaunchInfo* info);
+                            int zchunk_override, int flip_y,
+                            cudaStream_t stream, unsigned* dev_err,
+                            LaunchInfo* info);
 int tma_box_x(int dtype);
 int tma_box_y(int variant);
 
 // One time step with the generic kernel (any shape, any alignment).
 cudaError_t launch_step_generic(const void* f1, void* f2, int nx, int ny,
                                 int nz, const void* coef, int dtype,
-                                cudaStream_t stream, LaunchInfo* info);
+                                int flip_y, cudaStream_t stream,
+                                LaunchInfo* info);
+
+// One 2D 5-point time step (diffusion::Diffusion with nd = 2), any shape
+// and alignment; ychunk_override = rows per warp task (0 = automatic).
+struct Step2dVariant {
+  int ring;  // rows in each lane's register ring
+};
+constexpr int kNumStep2dVariants = 6;
+extern const Step2dVariant kStep2dVariants[kNumStep2dVariants];
+int default_step2d_variant();
+cudaError_t launch_step2d(const void* f1, void* f2, int nx, int ny,
+                          const void* coef, int dtype, int variant,
+                          int ychunk_override, cudaStream_t stream,
+                          LaunchInfo* info);
+// The widest access (in values, 16 bytes at most) that nx and the buffers'
+// alignment allow; the 2D kernel uses vector accesses when it is 16 bytes.
+int step2d_vector_width(const void* f1, const void* f2, int nx, int dtype);
 
 // k fused time steps (temporal blocking), f2 = stencil^k(f1).
 cudaError_t launch_steps_tb(const CUtensorMap& src, void* f2, int nx, int ny,
                             int nz, const void* coef, int dtype, int k,
-                            int zchunk_override, cudaStream_t stream,
-                            unsigned* dev_err, LaunchInfo* info);
+                            int zchunk_override, int flip_y,
+                            cudaStream_t stream, unsigned* dev_err,
+                            LaunchInfo* info);
 int tb_box_x(int dtype, int k);
 int tb_box_y(int k);
 bool tb_supported(int k, int dtype);
@@ -106,10 +129,12 @@ cudaError_t launch_batch_step(int shape, const BatchDesc* descs,
 
 // FP64 error norms of a field against the analytic solution at `time`,
 // evaluated per point (no analytic buffer); result in scratch[0..3].
-cudaError_t launch_accuracy(const void* f, int dtype, int nx, int ny, int nz,
-                            double kx, double ky, double kz, double dx,
-                            double dy, double dz, double kappa, double time,
-                            double* scratch, cudaStream_t stream);
+// ndim = 2 drops the z factor (the 2D field of diffusion::Diffusion).
+cudaError_t launch_accuracy(const void* f, int dtype, int ndim, int nx,
+                            int ny, int nz, double kx, double ky, double kz,
+                            double dx, double dy, double dz, double kappa,
+                            double time, double* scratch,
+                            cudaStream_t stream);
 
 // A one-CTA kernel whose bounded mbarrier wait is bound to run out.
 cudaError_t launch_selftest_wait(unsigned limit, unsigned* dev_err,
@@ -117,9 +142,9 @@ cudaError_t launch_selftest_wait(unsigned limit, unsigned* dev_err,
 
 // Analytic solution (the reference's Initialize, computed in FP64 on the
 // device) written in `dtype` at `time`.
-cudaError_t launch_analytic(void* out, int dtype, int nx, int ny, int nz,
-                            double kx, double ky, double kz, double dx,
-                            double dy, double dz, double kappa, double time,
-                            cudaStream_t stream);
+cudaError_t launch_analytic(void* out, int dtype, int ndim, int nx, int ny,
+                            int nz, double kx, double ky, double kz,
+                            double dx, double dy, double dz, double kappa,
+                            double time, cudaStream_t stream);
 
 }  // namespace d3d

@@ -39,7 +39,8 @@ __device__ __forceinline__ void march_tile(const T* __restrict__ src,
                                            T* __restrict__ dst, int nx,
                                            int ny, int nz, int x0, int y0,
                                            int z0, int z1, const Coef<T>& k,
-                                           T (*stage)[MarchTile<BX, BY>::E]) {
+                                           T (*stage)[MarchTile<BX, BY>::E],
+                                           bool flip_y = false) {
   using TL = MarchTile<BX, BY>;
   const int tid = threadIdx.x;
   const int tx = tid % BX, ty = tid / BX;
@@ -69,6 +70,9 @@ __device__ __forceinline__ void march_tile(const T* __restrict__ src,
   const int halo_g = hy * nx + hx;
   const bool store_ok = xg < nx && yg < ny;
   const size_t plane = (size_t)nx * ny;
+  // n is y-1 and s is y+1 (diffusion3d); flip_y swaps them for the
+  // diffusion::Diffusion order, where the y-1 term is summed first.
+  const int nrow = flip_y ? -TL::W : TL::W;
 
   // Load pointers step one plane per call and stop at the last plane the
   // chunk needs (plane z1 is the t of plane z1-1); later calls re-read it.
@@ -107,8 +111,8 @@ __device__ __forceinline__ void march_tile(const T* __restrict__ src,
     __syncthreads();
     const T w = st[own_s - 1];
     const T e = st[own_s + 1];
-    const T n = st[own_s - TL::W];
-    const T s = st[own_s + TL::W];
+    const T n = st[own_s - nrow];
+    const T s = st[own_s + nrow];
     const T v = point(k, c, w, e, s, n, b, t);
     if (store_ok) *out = v;
     out += plane;
@@ -159,7 +163,7 @@ template <int BX, int BY>
 __device__ __forceinline__ void march_tile2(
     const float* __restrict__ src, float* __restrict__ dst, int nx, int ny,
     int nz, int x0, int y0, int z0, int z1, const Coef<float>& k,
-    float (*stage)[MarchTile2<BX, BY>::E]) {
+    float (*stage)[MarchTile2<BX, BY>::E], bool flip_y = false) {
   using TL = MarchTile2<BX, BY>;
   const int tid = threadIdx.x;
   const int tx = tid % TL::TX, ty = tid / TL::TX;
@@ -190,6 +194,7 @@ __device__ __forceinline__ void march_tile2(
   const bool store1 = xg + 1 < nx && yg < ny;
   const size_t plane = (size_t)nx * ny;
   const Coef2 kk = coef2(k);
+  const int nrow = flip_y ? -TL::W : TL::W;  // as in march_tile
 
   const int plim = min(z1, nz - 1);
   int pn = z0;
@@ -227,8 +232,8 @@ __device__ __forceinline__ void march_tile2(
     __syncthreads();
     const float w0 = st[own_s - 1];
     const float e1 = st[own_s + 2];
-    const float2 n = *reinterpret_cast<const float2*>(st + own_s - TL::W);
-    const float2 sv = *reinterpret_cast<const float2*>(st + own_s + TL::W);
+    const float2 n = *reinterpret_cast<const float2*>(st + own_s - nrow);
+    const float2 sv = *reinterpret_cast<const float2*>(st + own_s + nrow);
     const uint64_t r = point2(kk, pack2(c0, c1), pack2(w0, c0),
                               pack2(c1, e1), pack2(sv.x, sv.y),
                               pack2(n.x, n.y), b01, t01);

@@ -312,13 +312,15 @@ cudaError_t launch_compare(const void* a, int a_dtype, const void* b,
   return cudaGetLastError();
 }
 
-cudaError_t launch_accuracy(const void* f, int dtype, int nx, int ny, int nz,
-                            double kx, double ky, double kz, double dx,
-                            double dy, double dz, double kappa, double time,
-                            double* scratch, cudaStream_t stream) {
+cudaError_t launch_accuracy(const void* f, int dtype, int ndim, int nx,
+                            int ny, int nz, double kx, double ky, double kz,
+                            double dx, double dy, double dz, double kappa,
+                            double time, double* scratch,
+                            cudaStream_t stream) {
   const double ax = exp(-kappa * time * (kx * kx));
   const double ay = exp(-kappa * time * (ky * ky));
-  const double az = exp(-kappa * time * (kz * kz));
+  // A 2D field has no z factor: az = 0 makes it exactly 1.
+  const double az = ndim == 2 ? 0.0 : exp(-kappa * time * (kz * kz));
   double* partial = scratch + 4;
   if (dtype == kF64)
     accuracy_partial_kernel<double><<<kCmpBlocks, kCmpThreads, 0, stream>>>(
@@ -341,13 +343,13 @@ cudaError_t launch_selftest_wait(unsigned limit, unsigned* dev_err,
   return cudaGetLastError();
 }
 
-cudaError_t launch_analytic(void* out, int dtype, int nx, int ny, int nz,
-                            double kx, double ky, double kz, double dx,
-                            double dy, double dz, double kappa, double time,
-                            cudaStream_t stream) {
+cudaError_t launch_analytic(void* out, int dtype, int ndim, int nx, int ny,
+                            int nz, double kx, double ky, double kz,
+                            double dx, double dy, double dz, double kappa,
+                            double time, cudaStream_t stream) {
   const double ax = exp(-kappa * time * (kx * kx));
   const double ay = exp(-kappa * time * (ky * ky));
-  const double az = exp(-kappa * time * (kz * kz));
+  const double az = ndim == 2 ? 0.0 : exp(-kappa * time * (kz * kz));
   const int threads = 256, blocks = 148 * 8;
   if (dtype == kF64)
     analytic_kernel<double><<<blocks, threads, 0, stream>>>(

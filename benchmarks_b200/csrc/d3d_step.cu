@@ -55,7 +55,7 @@ template <typename T, int BY, int S>
 __global__ void __launch_bounds__(StepTmaCfg<T, BY, S>::THREADS)
     step_tma_kernel(const __grid_constant__ CUtensorMap src,
                     T* __restrict__ dst, int nx, int ny, int nz, Coef<T> k,
-                    int zchunk, unsigned* __restrict__ dev_err) {
+                    int zchunk, int flip_y, unsigned* __restrict__ dev_err) {
   using C = StepTmaCfg<T, BY, S>;
   constexpr int V = C::V;
   constexpr int RPW = C::RPW;
@@ -114,6 +114,11 @@ __global__ void __launch_bounds__(StepTmaCfg<T, BY, S>::THREADS)
     s_off[r] = (yg >= ny - 1) ? c_off[r] : (row + 2) * C::P + col;
     g_off[r] = (size_t)yg * nx + xg;
     store_ok[r] = (yg < ny) && (xg < nx);
+    if (flip_y) {  // diffusion::Diffusion order: the y-1 term is summed 4th
+      const int t = n_off[r];
+      n_off[r] = s_off[r];
+      s_off[r] = t;
+    }
   }
   const int wl_adj = (xg == 0) ? 0 : -1;  // lane 0's w load
   const size_t plane = (size_t)nx * ny;
@@ -226,34 +231,38 @@ template <> struct GenTile<double> { static constexpr int BX = 32, BY = 8; };
 template <typename T>
 __global__ void __launch_bounds__(256)
     step_generic_kernel(const T* __restrict__ src, T* __restrict__ dst,
-                        int nx, int ny, int nz, Coef<T> k, int zchunk);
+                        int nx, int ny, int nz, Coef<T> k, int zchunk,
+                        int flip_y);
 
 template <>
 __global__ void __launch_bounds__(256)
     step_generic_kernel<float>(const float* __restrict__ src,
                                float* __restrict__ dst, int nx, int ny,
-                               int nz, Coef<float> k, int zchunk) {
+                               int nz, Coef<float> k, int zchunk,
+                               int flip_y) {
   constexpr int BX = GenTile<float>::BX, BY = GenTile<float>::BY;
   __shared__ __align__(16) float stage[2][MarchTile2<BX, BY>::E];
   const int z0 = blockIdx.z * zchunk;
   const int z1 = min(nz, z0 + zchunk);
   if (z0 >= z1) return;
   march_tile2<BX, BY>(src, dst, nx, ny, nz, blockIdx.x * BX, blockIdx.y * BY,
-                      z0, z1, k, stage);
+                      z0, z1, k, stage, flip_y != 0);
 }
 
 template <>
 __global__ void __launch_bounds__(256)
     step_generic_kernel<double>(const double* __restrict__ src,
                                 double* __restrict__ dst, int nx, int ny,
-                                int nz, Coef<double> k, int zchunk) {
+                                int nz, Coef<double> k, int zchunk,
+                                int flip_y) {
   constexpr int BX = GenTile<double>::BX, BY = GenTile<double>::BY;
   __shared__ double stage[2][MarchTile<BX, BY>::E];
   const int z0 = blockIdx.z * zchunk;
   const int z1 = min(nz, z0 + zchunk);
   if (z0 >= z1) return;
   march_tile<double, BX, BY>(src, dst, nx, ny, nz, blockIdx.x * BX,
-                             blockIdx.y * BY, z0, z1, k, stage);
+                             blockIdx.y * BY, z0, z1, k, stage,
+                             flip_y != 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -306,7 +315,7 @@ int pick_zchunk(int nz, long tiles, int ctas_per_sm, int min_chunk) {
 template <typename T, int BY, int S>
 cudaError_t launch_tma_t(const CUtensorMap& src, void* f2, int nx, int ny,
                          int nz, const void* coef, int zchunk_override,
-                         cudaStream_t stream, unsigned* dev_err,
+                         int flip_y, cudaStream_t stream, unsigned* dev_err,
                          LaunchInfo* info) {
   using C = StepTmaCfg<T, BY, S>;
   auto kern = step_tma_kernel<T, BY, S>;
@@ -329,22 +338,23 @@ cudaError_t launch_tma_t(const CUtensorMap& src, void* f2, int nx, int ny,
   if (info) *info = LaunchInfo{gx, gy, gz, C::THREADS, C::SMEM, zchunk, occ};
   kern<<<dim3(gx, gy, gz), C::THREADS, C::SMEM, stream>>>(
       src, static_cast<T*>(f2), nx, ny, nz, coef_from<T>(coef), zchunk,
-      dev_err);
+      flip_y, dev_err);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_tma_dtype(const CUtensorMap& src, void* f2, int nx, int ny,
                              int nz, const void* coef, int variant,
-                             int zchunk_override, cudaStream_t stream,
-                             unsigned* dev_err, LaunchInfo* info) {
+                             int zchunk_override, int flip_y,
+                             cudaStream_t stream, unsigned* dev_err,
+                             LaunchInfo* info) {
   switch (variant) {
-    case 0: return launch_tma_t<T, 32, 4>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
-    case 1: return launch_tma_t<T, 16, 4>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
-    case 2: return launch_tma_t<T, 8, 4>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
-    case 3: return launch_tma_t<T, 16, 6>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
-    case 4: return launch_tma_t<T, 32, 6>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
-    case 5: return launch_tma_t<T, 8, 8>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
+    case 0: return launch_tma_t<T, 32, 4>(src, f2, nx, ny, nz, coef, zchunk_override, flip_y, stream, dev_err, info);
+    case 1: return launch_tma_t<T, 16, 4>(src, f2, nx, ny, nz, coef, zchunk_override, flip_y, stream, dev_err, info);
+    case 2: return launch_tma_t<T, 8, 4>(src, f2, nx, ny, nz, coef, zchunk_override, flip_y, stream, dev_err, info);
+    case 3: return launch_tma_t<T, 16, 6>(src, f2, nx, ny, nz, coef, zchunk_override, flip_y, stream, dev_err, info);
+    case 4: return launch_tma_t<T, 32, 6>(src, f2, nx, ny, nz, coef, zchunk_override, flip_y, stream, dev_err, info);
+    case 5: return launch_tma_t<T, 8, 8>(src, f2, nx, ny, nz, coef, zchunk_override, flip_y, stream, dev_err, info);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -394,18 +404,22 @@ cudaError_t encode_field_map(CUtensorMap* map, const void* ptr, int nx, int ny,
 
 cudaError_t launch_step_tma(const CUtensorMap& src, void* f2, int nx, int ny,
                             int nz, const void* coef, int dtype, int variant,
-                            int zchunk_override, cudaStream_t stream,
-                            unsigned* dev_err, LaunchInfo* info) {
+                            int zchunk_override, int flip_y,
+                            cudaStream_t stream, unsigned* dev_err,
+                            LaunchInfo* info) {
   if (dtype == kF64)
     return launch_tma_dtype<double>(src, f2, nx, ny, nz, coef, variant,
-                                    zchunk_override, stream, dev_err, info);
+                                    zchunk_override, flip_y, stream, dev_err,
+                                    info);
   return launch_tma_dtype<float>(src, f2, nx, ny, nz, coef, variant,
-                                 zchunk_override, stream, dev_err, info);
+                                 zchunk_override, flip_y, stream, dev_err,
+                                 info);
 }
 
 cudaError_t launch_step_generic(const void* f1, void* f2, int nx, int ny,
                                 int nz, const void* coef, int dtype,
-                                cudaStream_t stream, LaunchInfo* info) {
+                                int flip_y, cudaStream_t stream,
+                                LaunchInfo* info) {
   const int bx = dtype == kF64 ? GenTile<double>::BX : GenTile<float>::BX;
   const int by = dtype == kF64 ? GenTile<double>::BY : GenTile<float>::BY;
   const int gx = (nx + bx - 1) / bx;
@@ -417,11 +431,11 @@ cudaError_t launch_step_generic(const void* f1, void* f2, int nx, int ny,
   if (dtype == kF64)
     step_generic_kernel<double><<<grid, block, 0, stream>>>(
         static_cast<const double*>(f1), static_cast<double*>(f2), nx, ny, nz,
-        coef_from<double>(coef), zchunk);
+        coef_from<double>(coef), zchunk, flip_y);
   else
     step_generic_kernel<float><<<grid, block, 0, stream>>>(
         static_cast<const float*>(f1), static_cast<float*>(f2), nx, ny, nz,
-        coef_from<float>(coef), zchunk);
+        coef_from<float>(coef), zchunk, flip_y);
   return cudaGetLastError();
 }
 

@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(TbCfg<T, K, BY, S0>::THREADS,
                                   TbCfg<T, K, BY, S0>::MIN_CTAS)
     steps_tb_kernel(const __grid_constant__ CUtensorMap src,
                     T* __restrict__ dst, int nx, int ny, int nz, Coef<T> k,
-                    int zchunk, unsigned* __restrict__ dev_err) {
+                    int zchunk, int flip_y, unsigned* __restrict__ dev_err) {
   using C = TbCfg<T, K, BY, S0>;
   constexpr int V = C::V;
   constexpr int P = C::P;
@@ -150,6 +150,11 @@ __global__ void __launch_bounds__(TbCfg<T, K, BY, S0>::THREADS,
     c_off[i] = r * P + col;
     n_off[i] = (yg == 0 ? r : r - 1) * P + col;
     s_off[i] = (yg == ny - 1 ? r : r + 1) * P + col;
+    if (flip_y) {  // diffusion::Diffusion order: the y-1 term is summed 4th
+      const int t = n_off[i];
+      n_off[i] = s_off[i];
+      s_off[i] = t;
+    }
     w_off[i] = r * P + (xg == 0 ? col : max(col - 1, 0));
     e_off[i] = r * P + (xg + V - 1 == nx - 1 ? col + V - 1 : min(col + V, P - 1));
     g_off[i] = (size_t)(yg < 0 ? 0 : yg) * nx + (xg < 0 ? 0 : xg);
@@ -278,7 +283,7 @@ namespace {
 template <typename T, int K, int BY, int S0>
 cudaError_t launch_tb_t(const CUtensorMap& src, void* f2, int nx, int ny,
                         int nz, const void* coef, int zchunk_override,
-                        cudaStream_t stream, unsigned* dev_err,
+                        int flip_y, cudaStream_t stream, unsigned* dev_err,
                         LaunchInfo* info) {
   using C = TbCfg<T, K, BY, S0>;
   auto kern = steps_tb_kernel<T, K, BY, S0>;
@@ -304,7 +309,8 @@ cudaError_t launch_tb_t(const CUtensorMap& src, void* f2, int nx, int ny,
   const int gz = (nz + zchunk - 1) / zchunk;
   if (info) *info = LaunchInfo{gx, gy, gz, C::THREADS, C::SMEM, zchunk, occ};
   kern<<<dim3(gx, gy, gz), C::THREADS, C::SMEM, stream>>>(
-      src, static_cast<T*>(f2), nx, ny, nz, coef_from<T>(coef), zchunk, dev_err);
+      src, static_cast<T*>(f2), nx, ny, nz, coef_from<T>(coef), zchunk, flip_y,
+      dev_err);
   return cudaGetLastError();
 }
 
@@ -316,12 +322,12 @@ template <> struct TbShape<4> { static constexpr int BY = 8, S0 = 5; };
 
 template <typename T>
 cudaError_t launch_tb_dtype(const CUtensorMap& src, void* f2, int nx, int ny,
-                            int nz, const void* coef, int k, int zc,
+                            int nz, const void* coef, int k, int zc, int fy,
                             cudaStream_t s, unsigned* err, LaunchInfo* info) {
   switch (k) {
-    case 2: return launch_tb_t<T, 2, TbShape<2>::BY, TbShape<2>::S0>(src, f2, nx, ny, nz, coef, zc, s, err, info);
-    case 3: return launch_tb_t<T, 3, TbShape<3>::BY, TbShape<3>::S0>(src, f2, nx, ny, nz, coef, zc, s, err, info);
-    case 4: return launch_tb_t<T, 4, TbShape<4>::BY, TbShape<4>::S0>(src, f2, nx, ny, nz, coef, zc, s, err, info);
+    case 2: return launch_tb_t<T, 2, TbShape<2>::BY, TbShape<2>::S0>(src, f2, nx, ny, nz, coef, zc, fy, s, err, info);
+    case 3: return launch_tb_t<T, 3, TbShape<3>::BY, TbShape<3>::S0>(src, f2, nx, ny, nz, coef, zc, fy, s, err, info);
+    case 4: return launch_tb_t<T, 4, TbShape<4>::BY, TbShape<4>::S0>(src, f2, nx, ny, nz, coef, zc, fy, s, err, info);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -349,13 +355,15 @@ int tb_box_y(int k) {
 
 cudaError_t launch_steps_tb(const CUtensorMap& src, void* f2, int nx, int ny,
                             int nz, const void* coef, int dtype, int k,
-                            int zchunk_override, cudaStream_t stream,
-                            unsigned* dev_err, LaunchInfo* info) {
+                            int zchunk_override, int flip_y,
+                            cudaStream_t stream, unsigned* dev_err,
+                            LaunchInfo* info) {
   if (dtype == kF64)
     return launch_tb_dtype<double>(src, f2, nx, ny, nz, coef, k,
-                                   zchunk_override, stream, dev_err, info);
+                                   zchunk_override, flip_y, stream, dev_err,
+                                   info);
   return launch_tb_dtype<float>(src, f2, nx, ny, nz, coef, k, zchunk_override,
-                                stream, dev_err, info);
+                                flip_y, stream, dev_err, info);
 }
 
 }  // namespace d3d

@@ -1,12 +1,14 @@
 """A small, fixed workload for profiling one kernel under ncu.
 
     python -m benchmarks_b200.profile --kernel tma --n 512 --steps 4
+    python -m benchmarks_b200.profile --kernel step2d --n 16384 --steps 4
 
 Runs `steps` time steps of one kernel on an n^3 FP32 (or FP64) field of
 uniform random values through the C ABI and exits.  With n = 512 each FP32
 buffer is 512 MiB (larger than the 126 MB L2), two buffers in all.
-Kernels: tma, generic, tb2, tb3, tb4 (temporal blocking), and the same
-names with an f64_ prefix.
+Kernels: tma, generic, tb2, tb3, tb4 (temporal blocking), step2d (an n^2
+grid of the diffusion::Diffusion surface; n = 16384 gives 1 GiB buffers),
+and the same names with an f64_ prefix.
 """
 from __future__ import annotations
 
@@ -20,6 +22,7 @@ KERNELS = {
     "tb2": (B.KERNEL_TB, 2),
     "tb3": (B.KERNEL_TB, 3),
     "tb4": (B.KERNEL_TB, 4),
+    "step2d": (B.KERNEL_AUTO, 1),
 }
 
 
@@ -39,17 +42,21 @@ def main():
         name = name[4:]
     kernel, tb = KERNELS[name]
     n = args.n
-    plan = B.Plan(n, n, n, dtype, kernel, tb, variant=args.variant,
-                  zchunk=args.zchunk)
+    if name == "step2d":
+        plan = B.DiffusionPlan((n, n), dtype, kernel, zchunk=args.zchunk)
+    else:
+        plan = B.Plan(n, n, n, dtype, kernel, tb, variant=args.variant,
+                      zchunk=args.zchunk)
     gen = torch.Generator(device="cuda").manual_seed(7)
     tdt = torch.float64 if dtype == B.F64 else torch.float32
-    f1 = torch.rand((n, n, n), device="cuda", generator=gen, dtype=tdt)
+    f1 = torch.rand(plan.shape, device="cuda", generator=gen, dtype=tdt)
     f2 = torch.empty_like(f1)
     plan.run(f1, f2, args.steps)
     torch.cuda.synchronize()
     flags = B.check_device_errors()
-    print("profile case done: %s %d^3 x %d steps, %s, device flags %d"
-          % (args.kernel, n, args.steps, plan.info()["last_kernel"], flags))
+    print("profile case done: %s n=%d (%dD) x %d steps, %s, device flags %d"
+          % (args.kernel, n, plan.ndim, args.steps,
+             plan.info()["last_kernel"], flags))
 
 
 if __name__ == "__main__":

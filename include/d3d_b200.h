@@ -75,8 +75,38 @@ int d3d_coefficients(int nx, int ny, int nz, int dtype, void* coeff7,
 int d3d_plan_create(int nx, int ny, int nz, int dtype, int kernel,
                     int tb_depth, d3d_plan* out);
 
+/* ---------------------------------------------------------------------
+ * The reference's second plugin surface, diffusion::Diffusion
+ * (src/diffusion/diffusion.h:80-180): nd = 2 (5-point, nx*ny) or nd = 3
+ * (7-point) grids, dims = {nx, ny[, nz]} as its constructor
+ * Diffusion(int ndim, const int* dims) takes them (diffusion.h:93-108).
+ * Two arithmetic differences from diffusion3d, both reproduced:
+ *   - cc = 1.0 - (ce + cw + cn + cs + (nd == 3 ? ct + cb : 0))
+ *     (diffusion.h:107), which can round differently from diffusion3d's;
+ *   - the y-1 neighbour is summed before y+1: f = cc*c + cw*w + ce*e +
+ *     cs*s + cn*n [+ cb*b + ct*t] with s = y-1, n = y+1
+ *     (diffusion_openmp.cc:71-74, 98-103).
+ * ------------------------------------------------------------------- */
+
+/* The coefficients and geometry diffusion::Diffusion derives for an nd-D
+ * grid (ct, cb and dz are those of a one-plane z axis when nd = 2 and go
+ * unused).  Same output layout as d3d_coefficients. */
+int d3d_diffusion_coefficients(int nd, const int* dims, int dtype,
+                               void* coeff7, void* geom8);
+
+/* A plan for a diffusion::Diffusion grid: the launch state
+ * DiffusionCUDA keeps (diffusion_cuda.h:44-59).  Every d3d_plan entry point
+ * below works on it (step, run, run_host, autotune, analytic, compare,
+ * accuracy).  nd = 3 runs the 3D kernels in this surface's order and takes
+ * any kernel; nd = 2 runs the 2D register-march kernel and takes
+ * D3D_KERNEL_AUTO or D3D_KERNEL_GENERIC (D3D_E_UNSUPPORTED otherwise). */
+int d3d_diffusion_plan_create(int nd, const int* dims, int dtype, int kernel,
+                              int tb_depth, d3d_plan* out);
+
 /* Overrides the tile variant (0..D3D_NUM_TILE_VARIANTS-1) and z-chunk
- * (planes per CTA, 0 = automatic) of a plan; used by the autotuner. */
+ * (planes per CTA, 0 = automatic) of a plan; used by the autotuner.  On a
+ * 2D plan the variant picks the 2D kernel's register-ring depth and L2
+ * prefetch distance, and zchunk is the rows per warp task. */
 #define D3D_NUM_TILE_VARIANTS 6
 int d3d_plan_set_tile(d3d_plan plan, int variant, int zchunk);
 
@@ -93,8 +123,8 @@ int d3d_plan_set_graphs(d3d_plan plan, int enable);
  * a set of z-chunk lengths over `steps` time steps on the caller's buffers
  * f1/f2 (their contents are overwritten) with CUDA events on `stream`, and
  * keeps the fastest in the plan.  For D3D_KERNEL_TB plans it tunes the
- * z-chunk of the fused passes.  *best_ms (may be NULL) receives the best
- * time per step. */
+ * z-chunk of the fused passes, for 2D plans the rows per warp task.
+ * *best_ms (may be NULL) receives the best time per step. */
 int d3d_plan_autotune(d3d_plan plan, void* f1, void* f2, const void* coeff,
                       int steps, void* stream, double* best_ms);
 

@@ -56,3 +56,36 @@ def test_plan_create_rejects_bad_arguments():
                              ctypes.byref(h)) == B.D3D_E_INVALID
     assert L.d3d_step(None, None, None, None, None) == B.D3D_E_INVALID
     assert L.d3d_run(None, None, None, None, 1, None) == B.D3D_E_INVALID
+
+
+@pytest.mark.parametrize("nd,dims", [(2, (256, 256)), (2, (37, 23)),
+                                     (2, (1, 1)), (3, (64, 64, 64)),
+                                     (3, (17, 23, 5)), (3, (24, 40, 16))])
+def test_diffusion_coefficients_match_oracle(nd, dims):
+    """diffusion::Diffusion's constructor (its cc sums the z pair as a unit)
+    through d3d_diffusion_coefficients, against the pinned restatement."""
+    nz = dims[2] if nd == 3 else 1
+    for dt, npdt in ((B.F32, np.float32), (B.F64, np.float64)):
+        c, g = B.diffusion_coefficients(nd, dims, dt)
+        oc, og = O.dif_params(nd, dims[0], dims[1], nz, npdt)
+        assert c.tobytes() == oc.tobytes()
+        assert g.tobytes() == og.tobytes()
+
+
+def test_diffusion_plan_rejects_bad_arguments():
+    h = ctypes.c_void_p()
+    L = B.lib()
+    d2 = (ctypes.c_int * 2)(16, 16)
+    d3 = (ctypes.c_int * 3)(16, 16, 0)
+    assert L.d3d_diffusion_plan_create(4, d2, B.F32, 0, 1,
+                                       ctypes.byref(h)) == B.D3D_E_INVALID
+    assert L.d3d_diffusion_plan_create(2, None, B.F32, 0, 1,
+                                       ctypes.byref(h)) == B.D3D_E_INVALID
+    assert L.d3d_diffusion_plan_create(3, d3, B.F32, 0, 1,
+                                       ctypes.byref(h)) == B.D3D_E_INVALID
+    for kernel in (B.KERNEL_TMA, B.KERNEL_TB):
+        assert L.d3d_diffusion_plan_create(2, d2, B.F32, kernel, 2,
+                                           ctypes.byref(h)) \
+            == B.D3D_E_UNSUPPORTED
+    assert L.d3d_diffusion_coefficients(1, d2, B.F32, None, None) \
+        == B.D3D_E_INVALID
