@@ -283,6 +283,43 @@ def serving_leg(B, torch, n_req=96, arena_gb=24.0, chunk=8):
             "p99_ratio_plain_over_served": plain["p99_ms"] / served["p99_ms"]}
 
 
+def diffusion2d_leg(B, torch, stream, side_n=16384, count=50, reps=4):
+    """The second plugin surface's 2D 5-point grid (diffusion::Diffusion,
+    nd = 2): device rate of the register-march kernel at side_n^2 (1 GiB
+    per FP32 buffer, larger than L2), FP32 and FP64, with the FP64
+    device accuracy report of a run from the analytic field."""
+    peak, _ = measured_peak_gbs()
+    out = {"grid": [side_n, side_n], "steps_per_run": count}
+    for dtype, name, es in ((B.F32, "f32", 4), (B.F64, "f64", 8)):
+        plan = B.DiffusionPlan((side_n, side_n), dtype)
+        a, b = plan.empty(), plan.empty()
+        plan.analytic(a, 0.0)
+        c = plan.reference_coefficients()
+        a, b = plan.run(a, b, count, c, stream)  # warm-up (graph capture)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            a, b = plan.run(a, b, count, c, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        rate = float(side_n) ** 2 * count * reps / t / 1e9
+        acc = plan.accuracy(a, count * (reps + 1), stream)
+        info = plan.info()
+        out[name] = {"value": rate, "unit": UNIT,
+                     "hbm_frac": rate * 2 * es / peak,
+                     "rms_vs_analytic": acc[0],
+                     "kernel": info["last_kernel"],
+                     "variant": info["variant"],
+                     "rows_per_task": info["launch_zchunk"]}
+        del a, b
+        plan.close()
+        torch.cuda.empty_cache()
+    return out
+
+
 def run_reference_arm(args):
     rank, world, _ = env_rank()
     if rank != 0:
@@ -517,6 +554,8 @@ def run_b200(args):
         side["batched"] = batched_leg(B, torch)
         torch.cuda.empty_cache()
         side["serving"] = serving_leg(B, torch)
+        torch.cuda.empty_cache()
+        side["diffusion2d"] = diffusion2d_leg(B, torch, stream)
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_reference_leg(n)
     if rank == 0:
@@ -535,7 +574,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true",
                     help="skip the CPU baseline leg")
     ap.add_argument("--no-side", action="store_true",
-                    help="skip the batched and serving legs")
+                    help="skip the batched, serving and 2D legs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -34,13 +34,14 @@ struct MarchPair {
   T own, halo;
 };
 
-template <typename T, int BX, int BY>
+// FLIP: the y-1 neighbour is summed before y+1 (diffusion::Diffusion)
+// instead of after it (diffusion3d).
+template <typename T, int BX, int BY, bool FLIP = false>
 __device__ __forceinline__ void march_tile(const T* __restrict__ src,
                                            T* __restrict__ dst, int nx,
                                            int ny, int nz, int x0, int y0,
                                            int z0, int z1, const Coef<T>& k,
-                                           T (*stage)[MarchTile<BX, BY>::E],
-                                           bool flip_y = false) {
+                                           T (*stage)[MarchTile<BX, BY>::E]) {
   using TL = MarchTile<BX, BY>;
   const int tid = threadIdx.x;
   const int tx = tid % BX, ty = tid / BX;
@@ -70,9 +71,8 @@ __device__ __forceinline__ void march_tile(const T* __restrict__ src,
   const int halo_g = hy * nx + hx;
   const bool store_ok = xg < nx && yg < ny;
   const size_t plane = (size_t)nx * ny;
-  // n is y-1 and s is y+1 (diffusion3d); flip_y swaps them for the
-  // diffusion::Diffusion order, where the y-1 term is summed first.
-  const int nrow = flip_y ? -TL::W : TL::W;
+  // n is y-1 and s is y+1 (diffusion3d); FLIP swaps them.
+  constexpr int nrow = FLIP ? -TL::W : TL::W;
 
   // Load pointers step one plane per call and stop at the last plane the
   // chunk needs (plane z1 is the t of plane z1-1); later calls re-read it.
@@ -159,11 +159,11 @@ struct MarchQuad {
   float o0, o1, halo;
 };
 
-template <int BX, int BY>
+template <int BX, int BY, bool FLIP = false>
 __device__ __forceinline__ void march_tile2(
     const float* __restrict__ src, float* __restrict__ dst, int nx, int ny,
     int nz, int x0, int y0, int z0, int z1, const Coef<float>& k,
-    float (*stage)[MarchTile2<BX, BY>::E], bool flip_y = false) {
+    float (*stage)[MarchTile2<BX, BY>::E]) {
   using TL = MarchTile2<BX, BY>;
   const int tid = threadIdx.x;
   const int tx = tid % TL::TX, ty = tid / TL::TX;
@@ -194,7 +194,7 @@ __device__ __forceinline__ void march_tile2(
   const bool store1 = xg + 1 < nx && yg < ny;
   const size_t plane = (size_t)nx * ny;
   const Coef2 kk = coef2(k);
-  const int nrow = flip_y ? -TL::W : TL::W;  // as in march_tile
+  constexpr int nrow = FLIP ? -TL::W : TL::W;  // as in march_tile
 
   const int plim = min(z1, nz - 1);
   int pn = z0;

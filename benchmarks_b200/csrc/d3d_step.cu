@@ -51,11 +51,13 @@ struct StepTmaCfg {
   static_assert(S >= 4, "the ring keeps planes z, z+1, z+2 and one in flight");
 };
 
-template <typename T, int BY, int S>
+// FLIP: sum the y-1 neighbour 4th and y+1 5th (diffusion::Diffusion)
+// instead of y+1 4th and y-1 5th (diffusion3d).
+template <typename T, int BY, int S, bool FLIP>
 __global__ void __launch_bounds__(StepTmaCfg<T, BY, S>::THREADS)
     step_tma_kernel(const __grid_constant__ CUtensorMap src,
                     T* __restrict__ dst, int nx, int ny, int nz, Coef<T> k,
-                    int zchunk, int flip_y, unsigned* __restrict__ dev_err) {
+                    int zchunk, unsigned* __restrict__ dev_err) {
   using C = StepTmaCfg<T, BY, S>;
   constexpr int V = C::V;
   constexpr int RPW = C::RPW;
@@ -114,7 +116,7 @@ __global__ void __launch_bounds__(StepTmaCfg<T, BY, S>::THREADS)
     s_off[r] = (yg >= ny - 1) ? c_off[r] : (row + 2) * C::P + col;
     g_off[r] = (size_t)yg * nx + xg;
     store_ok[r] = (yg < ny) && (xg < nx);
-    if (flip_y) {  // diffusion::Diffusion order: the y-1 term is summed 4th
+    if constexpr (FLIP) {
       const int t = n_off[r];
       n_off[r] = s_off[r];
       s_off[r] = t;
@@ -228,41 +230,23 @@ template <typename T> struct GenTile;
 template <> struct GenTile<float> { static constexpr int BX = 64, BY = 8; };
 template <> struct GenTile<double> { static constexpr int BX = 32, BY = 8; };
 
-template <typename T>
+template <typename T, bool FLIP>
 __global__ void __launch_bounds__(256)
     step_generic_kernel(const T* __restrict__ src, T* __restrict__ dst,
-                        int nx, int ny, int nz, Coef<T> k, int zchunk,
-                        int flip_y);
-
-template <>
-__global__ void __launch_bounds__(256)
-    step_generic_kernel<float>(const float* __restrict__ src,
-                               float* __restrict__ dst, int nx, int ny,
-                               int nz, Coef<float> k, int zchunk,
-                               int flip_y) {
-  constexpr int BX = GenTile<float>::BX, BY = GenTile<float>::BY;
-  __shared__ __align__(16) float stage[2][MarchTile2<BX, BY>::E];
+                        int nx, int ny, int nz, Coef<T> k, int zchunk) {
+  constexpr int BX = GenTile<T>::BX, BY = GenTile<T>::BY;
   const int z0 = blockIdx.z * zchunk;
   const int z1 = min(nz, z0 + zchunk);
   if (z0 >= z1) return;
-  march_tile2<BX, BY>(src, dst, nx, ny, nz, blockIdx.x * BX, blockIdx.y * BY,
-                      z0, z1, k, stage, flip_y != 0);
-}
-
-template <>
-__global__ void __launch_bounds__(256)
-    step_generic_kernel<double>(const double* __restrict__ src,
-                                double* __restrict__ dst, int nx, int ny,
-                                int nz, Coef<double> k, int zchunk,
-                                int flip_y) {
-  constexpr int BX = GenTile<double>::BX, BY = GenTile<double>::BY;
-  __shared__ double stage[2][MarchTile<BX, BY>::E];
-  const int z0 = blockIdx.z * zchunk;
-  const int z1 = min(nz, z0 + zchunk);
-  if (z0 >= z1) return;
-  march_tile<double, BX, BY>(src, dst, nx, ny, nz, blockIdx.x * BX,
-                             blockIdx.y * BY, z0, z1, k, stage,
-                             flip_y != 0);
+  if constexpr (sizeof(T) == 4) {
+    __shared__ __align__(16) float stage[2][MarchTile2<BX, BY>::E];
+    march_tile2<BX, BY, FLIP>(src, dst, nx, ny, nz, blockIdx.x * BX,
+                              blockIdx.y * BY, z0, z1, k, stage);
+  } else {
+    __shared__ double stage[2][MarchTile<BX, BY>::E];
+    march_tile<double, BX, BY, FLIP>(src, dst, nx, ny, nz, blockIdx.x * BX,
+                                     blockIdx.y * BY, z0, z1, k, stage);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -312,13 +296,13 @@ int pick_zchunk(int nz, long tiles, int ctas_per_sm, int min_chunk) {
   return (int)((nz + zs - 1) / zs);
 }
 
-template <typename T, int BY, int S>
+template <typename T, int BY, int S, bool FLIP>
 cudaError_t launch_tma_t(const CUtensorMap& src, void* f2, int nx, int ny,
                          int nz, const void* coef, int zchunk_override,
-                         int flip_y, cudaStream_t stream, unsigned* dev_err,
+                         cudaStream_t stream, unsigned* dev_err,
                          LaunchInfo* info) {
   using C = StepTmaCfg<T, BY, S>;
-  auto kern = step_tma_kernel<T, BY, S>;
+  auto kern = step_tma_kernel<T, BY, S, FLIP>;
   static bool attr_set = false;  // per instantiation; same on every device
   if (!attr_set) {
     cudaError_t e = cudaFuncSetAttribute(
@@ -338,23 +322,22 @@ cudaError_t launch_tma_t(const CUtensorMap& src, void* f2, int nx, int ny,
   if (info) *info = LaunchInfo{gx, gy, gz, C::THREADS, C::SMEM, zchunk, occ};
   kern<<<dim3(gx, gy, gz), C::THREADS, C::SMEM, stream>>>(
       src, static_cast<T*>(f2), nx, ny, nz, coef_from<T>(coef), zchunk,
-      flip_y, dev_err);
+      dev_err);
   return cudaGetLastError();
 }
 
-template <typename T>
+template <typename T, bool F>
 cudaError_t launch_tma_dtype(const CUtensorMap& src, void* f2, int nx, int ny,
                              int nz, const void* coef, int variant,
-                             int zchunk_override, int flip_y,
-                             cudaStream_t stream, unsigned* dev_err,
-                             LaunchInfo* info) {
+                             int zchunk_override, cudaStream_t stream,
+                             unsigned* dev_err, LaunchInfo* info) {
   switch (variant) {
-    case 0: return launch_tma_t<T, 32, 4>(src, f2, nx, ny, nz, coef, zchunk_override, flip_y, stream, dev_err, info);
-    case 1: return launch_tma_t<T, 16, 4>(src, f2, nx, ny, nz, coef, zchunk_override, flip_y, stream, dev_err, info);
-    case 2: return launch_tma_t<T, 8, 4>(src, f2, nx, ny, nz, coef, zchunk_override, flip_y, stream, dev_err, info);
-    case 3: return launch_tma_t<T, 16, 6>(src, f2, nx, ny, nz, coef, zchunk_override, flip_y, stream, dev_err, info);
-    case 4: return launch_tma_t<T, 32, 6>(src, f2, nx, ny, nz, coef, zchunk_override, flip_y, stream, dev_err, info);
-    case 5: return launch_tma_t<T, 8, 8>(src, f2, nx, ny, nz, coef, zchunk_override, flip_y, stream, dev_err, info);
+    case 0: return launch_tma_t<T, 32, 4, F>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
+    case 1: return launch_tma_t<T, 16, 4, F>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
+    case 2: return launch_tma_t<T, 8, 4, F>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
+    case 3: return launch_tma_t<T, 16, 6, F>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
+    case 4: return launch_tma_t<T, 32, 6, F>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
+    case 5: return launch_tma_t<T, 8, 8, F>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -407,13 +390,15 @@ cudaError_t launch_step_tma(const CUtensorMap& src, void* f2, int nx, int ny,
                             int zchunk_override, int flip_y,
                             cudaStream_t stream, unsigned* dev_err,
                             LaunchInfo* info) {
+  auto run = [&](auto fn) {
+    return fn(src, f2, nx, ny, nz, coef, variant, zchunk_override, stream,
+              dev_err, info);
+  };
   if (dtype == kF64)
-    return launch_tma_dtype<double>(src, f2, nx, ny, nz, coef, variant,
-                                    zchunk_override, flip_y, stream, dev_err,
-                                    info);
-  return launch_tma_dtype<float>(src, f2, nx, ny, nz, coef, variant,
-                                 zchunk_override, flip_y, stream, dev_err,
-                                 info);
+    return flip_y ? run(launch_tma_dtype<double, true>)
+                  : run(launch_tma_dtype<double, false>);
+  return flip_y ? run(launch_tma_dtype<float, true>)
+                : run(launch_tma_dtype<float, false>);
 }
 
 cudaError_t launch_step_generic(const void* f1, void* f2, int nx, int ny,
@@ -428,14 +413,24 @@ cudaError_t launch_step_generic(const void* f1, void* f2, int nx, int ny,
   const int gz = (nz + zchunk - 1) / zchunk;
   if (info) *info = LaunchInfo{gx, gy, gz, 256, 0, zchunk, 8};
   dim3 grid(gx, gy, gz), block(256);
-  if (dtype == kF64)
-    step_generic_kernel<double><<<grid, block, 0, stream>>>(
-        static_cast<const double*>(f1), static_cast<double*>(f2), nx, ny, nz,
-        coef_from<double>(coef), zchunk, flip_y);
-  else
-    step_generic_kernel<float><<<grid, block, 0, stream>>>(
-        static_cast<const float*>(f1), static_cast<float*>(f2), nx, ny, nz,
-        coef_from<float>(coef), zchunk, flip_y);
+  auto go = [&](auto kern, auto* a, auto* b, auto k) {
+    kern<<<grid, block, 0, stream>>>(a, b, nx, ny, nz, k, zchunk);
+  };
+  const double* d1 = static_cast<const double*>(f1);
+  const float* s1 = static_cast<const float*>(f1);
+  if (dtype == kF64) {
+    double* d2 = static_cast<double*>(f2);
+    if (flip_y)
+      go(step_generic_kernel<double, true>, d1, d2, coef_from<double>(coef));
+    else
+      go(step_generic_kernel<double, false>, d1, d2, coef_from<double>(coef));
+  } else {
+    float* s2 = static_cast<float*>(f2);
+    if (flip_y)
+      go(step_generic_kernel<float, true>, s1, s2, coef_from<float>(coef));
+    else
+      go(step_generic_kernel<float, false>, s1, s2, coef_from<float>(coef));
+  }
   return cudaGetLastError();
 }
 

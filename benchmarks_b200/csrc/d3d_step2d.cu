@@ -23,7 +23,7 @@
 //
 // Memory-level parallelism is what bounds the kernel: a lane's in-flight
 // rows cost registers, so the variants trade ring depth against occupancy
-// (kStep2dVariants), and short row chunks (8 rows by default) let each warp
+// (kStep2dVariants), and short row chunks (6 rows by default) let each warp
 // issue almost all of its loads at once.  Rows whose start is 16-byte
 // aligned (nx a multiple of 16 / sizeof(T), aligned buffers) use one vector
 // access per lane and row; other shapes keep the same 4 (FP32) or 2 (FP64)
@@ -246,14 +246,14 @@ cudaError_t launch2d_t(const void* f1, void* f2, int nx, int ny,
   const int nseg = (nx + 32 * V - 1) / (32 * V);
   int ychunk = ychunk_override;
   if (ychunk <= 0) {
-    // 8-row tasks (measured best on B200 from 4096^2 to 16384^2: a warp
-    // issues nearly all of a task's loads at once), shorter on grids too
-    // small to give each resident warp one.
+    // 6-row tasks (measured best on B200 from 4096^2 to 16384^2, FP32 and
+    // FP64: a warp issues nearly all of a task's loads at once), shorter on
+    // grids too small to give each resident warp one.
     const long long warps =
         (long long)sm_count() * ctas_per_sm * (kStep2dThreads / 32);
     const long long rows = (long long)ny * nseg;
     ychunk = (int)std::max<long long>(
-        2, std::min<long long>(8, (rows + warps - 1) / warps));
+        2, std::min<long long>(6, (rows + warps - 1) / warps));
   }
   ychunk = std::min(ychunk, ny);
   const long long nchunks = (ny + ychunk - 1) / ychunk;

@@ -79,12 +79,13 @@ struct TbCfg {
   static_assert(K >= 2 && K <= 4, "fusion depth");
 };
 
-template <typename T, int K, int BY, int S0>
+// FLIP: the y-1 neighbour is summed before y+1 (diffusion::Diffusion).
+template <typename T, int K, int BY, int S0, bool FLIP>
 __global__ void __launch_bounds__(TbCfg<T, K, BY, S0>::THREADS,
                                   TbCfg<T, K, BY, S0>::MIN_CTAS)
     steps_tb_kernel(const __grid_constant__ CUtensorMap src,
                     T* __restrict__ dst, int nx, int ny, int nz, Coef<T> k,
-                    int zchunk, int flip_y, unsigned* __restrict__ dev_err) {
+                    int zchunk, unsigned* __restrict__ dev_err) {
   using C = TbCfg<T, K, BY, S0>;
   constexpr int V = C::V;
   constexpr int P = C::P;
@@ -150,7 +151,7 @@ __global__ void __launch_bounds__(TbCfg<T, K, BY, S0>::THREADS,
     c_off[i] = r * P + col;
     n_off[i] = (yg == 0 ? r : r - 1) * P + col;
     s_off[i] = (yg == ny - 1 ? r : r + 1) * P + col;
-    if (flip_y) {  // diffusion::Diffusion order: the y-1 term is summed 4th
+    if constexpr (FLIP) {
       const int t = n_off[i];
       n_off[i] = s_off[i];
       s_off[i] = t;
@@ -286,7 +287,8 @@ cudaError_t launch_tb_t(const CUtensorMap& src, void* f2, int nx, int ny,
                         int flip_y, cudaStream_t stream, unsigned* dev_err,
                         LaunchInfo* info) {
   using C = TbCfg<T, K, BY, S0>;
-  auto kern = steps_tb_kernel<T, K, BY, S0>;
+  auto kern = flip_y ? steps_tb_kernel<T, K, BY, S0, true>
+                     : steps_tb_kernel<T, K, BY, S0, false>;
   cudaError_t e = cudaFuncSetAttribute(
       kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
   if (e != cudaSuccess) return e;
@@ -309,7 +311,7 @@ cudaError_t launch_tb_t(const CUtensorMap& src, void* f2, int nx, int ny,
   const int gz = (nz + zchunk - 1) / zchunk;
   if (info) *info = LaunchInfo{gx, gy, gz, C::THREADS, C::SMEM, zchunk, occ};
   kern<<<dim3(gx, gy, gz), C::THREADS, C::SMEM, stream>>>(
-      src, static_cast<T*>(f2), nx, ny, nz, coef_from<T>(coef), zchunk, flip_y,
+      src, static_cast<T*>(f2), nx, ny, nz, coef_from<T>(coef), zchunk,
       dev_err);
   return cudaGetLastError();
 }

@@ -1,0 +1,81 @@
+// DiffusionB200 over the C ABI (see diffusion_b200.h).
+#include "diffusion_b200.h"
+
+#include <stdio.h>
+#include <stdlib.h>
+
+namespace diffusion {
+
+namespace {
+
+// The reference's failure convention (FORCE_CHECK_CUDA, common/cuda_util.h:
+// 4-12): report and stop.
+void Check(int rc, const char* what) {
+  if (rc != D3D_OK) {
+    fprintf(stderr, "%s failed (%d): %s\n", what, rc, d3d_last_error());
+    exit(EXIT_FAILURE);
+  }
+}
+
+}  // namespace
+
+std::string DiffusionB200::GetName() const {
+  if (kernel_ == D3D_KERNEL_TB)
+    return std::string("b200_tb") + std::to_string(tb_depth_);
+  if (kernel_ == D3D_KERNEL_GENERIC) return "b200_generic";
+  return "b200";
+}
+
+std::string DiffusionB200::GetDescription() const {
+  return ndim_ == 2 ? "B200 sm_100a register-march 2D kernel"
+                    : "B200 sm_100a 3D kernels";
+}
+
+// As DiffusionCUDA::Setup (diffusion_cuda.cu:111-122): pinned host f1_, two
+// device buffers.
+void DiffusionB200::Setup() {
+  const size_t bytes = sizeof(REAL) * (size_t)nx_ * ny_ * nz_;
+  const int dtype = sizeof(REAL) == 8 ? D3D_F64 : D3D_F32;
+  const int dims[3] = {nx_, ny_, nz_};
+  Check(d3d_diffusion_plan_create(ndim_, dims, dtype, kernel_, tb_depth_,
+                                  &plan_),
+        "d3d_diffusion_plan_create");
+  void* host = nullptr;
+  Check(d3d_host_alloc(bytes, &host), "d3d_host_alloc");
+  f1_ = static_cast<REAL*>(host);
+  f2_ = nullptr;  // the second buffer lives on the device only
+  Check(d3d_device_alloc(bytes, &f1_d_), "d3d_device_alloc");
+  Check(d3d_device_alloc(bytes, &f2_d_), "d3d_device_alloc");
+}
+
+// As DiffusionCUDA::RunKernel (diffusion_cuda.cu:134-161): host f1_ in,
+// `count` steps on the device, result back in host f1_.
+void DiffusionB200::RunKernel(int count) {
+  const REAL coeff[7] = {ce_, cw_, cn_, cs_, ct_, cb_, cc_};
+  Check(d3d_run_host(plan_, f1_, f1_d_, f2_d_, coeff, count, nullptr,
+                     &kernel_ms_),
+        "d3d_run_host");
+}
+
+void DiffusionB200::FinalizeBenchmark() {
+  Check(d3d_host_free(f1_), "d3d_host_free");
+  f1_ = nullptr;
+  Check(d3d_device_free(f1_d_), "d3d_device_free");
+  Check(d3d_device_free(f2_d_), "d3d_device_free");
+  f1_d_ = f2_d_ = nullptr;
+  d3d_plan_destroy(plan_);
+  plan_ = nullptr;
+}
+
+// Baseline's report plus the kernel-only block of
+// DiffusionCUDA::DisplayResult (diffusion_cuda.cu:163-174).
+void DiffusionB200::DisplayResult(int count, float time) {
+  Baseline::DisplayResult(count, time);
+  const float t = kernel_ms_ * 1.0e-03f;
+  printf("Kernel-only performance:\n");
+  printf("Elapsed time : %.3f (s)\n", t);
+  printf("FLOPS        : %.3f (GFLOPS)\n", GetGFLOPS(count, t));
+  printf("Throughput   : %.3f (GB/s)\n", GetThroughput(count, t));
+}
+
+}  // namespace diffusion
