@@ -290,74 +290,90 @@ void drop_graphs(d3d_plan p) {
   }
 }
 
-// run_loop through a cached CUDA graph: the `count` launches of a
-// RunKernel-style loop are captured once and replayed as one graph launch,
-// which removes the per-launch host overhead and the gaps between steps.
-// Falls back to direct launches when the caller's stream is itself being
-// captured (the launches then land in the caller's graph).
-int run_graphed(d3d_plan p, void** f1, void** f2, const void* coeff,
-                int count, cudaStream_t s) {
+// The CUDA graph of a `count`-step run_loop on (f1, f2): found in the cache
+// or captured once (on the plan's own stream, so nothing runs) and
+// instantiated.  *out is null when graphs do not apply: disabled, fewer
+// than two steps, or `s` itself being captured (the launches then land in
+// the caller's graph).  Capture is host work only, so callers that time
+// the loop call this before their start event.
+int prepare_graph(d3d_plan p, void* f1, void* f2, const void* coeff,
+                  int count, cudaStream_t s, d3d_plan_s::GraphEntry** out) {
+  *out = nullptr;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   if (!p->use_graphs || count < 2 ||
       cudaStreamIsCapturing(s, &cap) != cudaSuccess ||
       cap != cudaStreamCaptureStatusNone)
-    return run_loop(p, f1, f2, coeff, count, s);
+    return D3D_OK;
   const size_t cb = 7 * d3d::dtype_size(p->dtype);
-  d3d_plan_s::GraphEntry* hit = nullptr;
   for (auto& g : p->graphs)
-    if (g.exec && g.f1 == *f1 && g.f2 == *f2 && g.count == count &&
+    if (g.exec && g.f1 == f1 && g.f2 == f2 && g.count == count &&
         g.variant == p->variant && g.zchunk == p->zchunk &&
         memcmp(g.coeff, coeff, cb) == 0) {
-      hit = &g;
-      break;
+      *out = &g;
+      return D3D_OK;
     }
-  if (!hit) {
-    if (!p->capture_stream)
-      D3D_TRY(cudaStreamCreateWithFlags(&p->capture_stream,
-                                        cudaStreamNonBlocking),
-              "cudaStreamCreateWithFlags");
-    auto& g = p->graphs[p->graph_next];
-    p->graph_next = (p->graph_next + 1) % 4;
-    if (g.exec) cudaGraphExecDestroy(g.exec);
-    g.exec = nullptr;
-    void* a = *f1;
-    void* b = *f2;
-    const unsigned long long l0 = g_launches.load();
-    D3D_TRY(cudaStreamBeginCapture(p->capture_stream,
-                                   cudaStreamCaptureModeThreadLocal),
-            "cudaStreamBeginCapture");
-    int rc = run_loop(p, &a, &b, coeff, count, p->capture_stream);
-    cudaGraph_t graph = nullptr;
-    cudaError_t e = cudaStreamEndCapture(p->capture_stream, &graph);
-    const unsigned long long captured = g_launches.load() - l0;
-    g_launches.fetch_sub(captured);  // counted when the graph runs
-    if (rc) {
-      if (graph) cudaGraphDestroy(graph);
-      return rc;
-    }
-    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
-    e = cudaGraphInstantiate(&g.exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) {
-      g.exec = nullptr;
-      return cuda_fail(e, "cudaGraphInstantiate");
-    }
-    g.f1 = *f1;
-    g.f2 = *f2;
-    g.count = count;
-    g.variant = p->variant;
-    g.zchunk = p->zchunk;
-    memcpy(g.coeff, coeff, cb);
-    g.result = a;
-    g.other = b;
-    g.launches = captured;
-    hit = &g;
+  if (!p->capture_stream)
+    D3D_TRY(cudaStreamCreateWithFlags(&p->capture_stream,
+                                      cudaStreamNonBlocking),
+            "cudaStreamCreateWithFlags");
+  auto& g = p->graphs[p->graph_next];
+  p->graph_next = (p->graph_next + 1) % 4;
+  if (g.exec) cudaGraphExecDestroy(g.exec);
+  g.exec = nullptr;
+  void* a = f1;
+  void* b = f2;
+  const unsigned long long l0 = g_launches.load();
+  D3D_TRY(cudaStreamBeginCapture(p->capture_stream,
+                                 cudaStreamCaptureModeThreadLocal),
+          "cudaStreamBeginCapture");
+  int rc = run_loop(p, &a, &b, coeff, count, p->capture_stream);
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(p->capture_stream, &graph);
+  const unsigned long long captured = g_launches.load() - l0;
+  g_launches.fetch_sub(captured);  // counted when the graph runs
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
   }
-  D3D_TRY(cudaGraphLaunch(hit->exec, s), "cudaGraphLaunch");
-  g_launches.fetch_add(hit->launches, std::memory_order_relaxed);
-  *f1 = hit->result;
-  *f2 = hit->other;
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&g.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    g.exec = nullptr;
+    return cuda_fail(e, "cudaGraphInstantiate");
+  }
+  g.f1 = f1;
+  g.f2 = f2;
+  g.count = count;
+  g.variant = p->variant;
+  g.zchunk = p->zchunk;
+  memcpy(g.coeff, coeff, cb);
+  g.result = a;
+  g.other = b;
+  g.launches = captured;
+  *out = &g;
   return D3D_OK;
+}
+
+int launch_graph(const d3d_plan_s::GraphEntry* g, void** f1, void** f2,
+                 cudaStream_t s) {
+  D3D_TRY(cudaGraphLaunch(g->exec, s), "cudaGraphLaunch");
+  g_launches.fetch_add(g->launches, std::memory_order_relaxed);
+  *f1 = g->result;
+  *f2 = g->other;
+  return D3D_OK;
+}
+
+// run_loop through a cached CUDA graph: the `count` launches of a
+// RunKernel-style loop are captured once and replayed as one graph launch,
+// which removes the per-launch host overhead and the gaps between steps.
+int run_graphed(d3d_plan p, void** f1, void** f2, const void* coeff,
+                int count, cudaStream_t s) {
+  d3d_plan_s::GraphEntry* g = nullptr;
+  int rc = prepare_graph(p, *f1, *f2, coeff, count, s, &g);
+  if (rc) return rc;
+  if (!g) return run_loop(p, f1, f2, coeff, count, s);
+  return launch_graph(g, f1, f2, s);
 }
 
 }  // namespace
@@ -419,7 +435,7 @@ int plan_new(int ndim, int flip_y, int nx, int ny, int nz, int dtype,
   p->kernel = kernel;
   p->tb_depth = kernel == D3D_KERNEL_TB ? tb_depth : 1;
   p->variant = ndim == 2 ? d3d::default_step2d_variant()
-                         : d3d::default_tma_variant(ny);
+                         : d3d::default_tma_variant(nx, ny, nz, dtype);
   p->zchunk = 0;
   p->device = dev;
   p->n = (size_t)nx * ny * nz;
@@ -659,12 +675,16 @@ int d3d_run_host(d3d_plan p, void* host_f1, void* dev_f1, void* dev_f2,
   if (rc) return rc;
   cudaStream_t s = as_stream(stream);
   const size_t bytes = p->n * d3d::dtype_size(p->dtype);
+  // Graph capture is one-off host setup; keep it out of the timed loop.
+  d3d_plan_s::GraphEntry* g = nullptr;
+  rc = prepare_graph(p, dev_f1, dev_f2, coeff, count, s, &g);
+  if (rc) return rc;
   D3D_TRY(cudaMemcpyAsync(dev_f1, host_f1, bytes, cudaMemcpyHostToDevice, s),
           "H2D copy");
   D3D_TRY(cudaEventRecord(p->ev[0], s), "cudaEventRecord");
   void* a = dev_f1;
   void* b = dev_f2;
-  rc = run_graphed(p, &a, &b, coeff, count, s);
+  rc = g ? launch_graph(g, &a, &b, s) : run_loop(p, &a, &b, coeff, count, s);
   if (rc) return rc;
   D3D_TRY(cudaEventRecord(p->ev[1], s), "cudaEventRecord");
   D3D_TRY(cudaMemcpyAsync(host_f1, a, bytes, cudaMemcpyDeviceToHost, s),

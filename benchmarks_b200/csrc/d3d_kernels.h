@@ -25,8 +25,8 @@ struct TmaVariant {
   int stages;  // planes in the shared-memory ring
 };
 constexpr int kNumTmaVariants = 6;
-// Default tile variant for a grid with `ny` rows.
-int default_tma_variant(int ny);
+// Default tile variant for an nx*ny*nz grid of `dtype`.
+int default_tma_variant(int nx, int ny, int nz, int dtype);
 const TmaVariant& tma_variant(int i);
 
 // Launch geometry actually used (for reporting and for the autotuner).

@@ -162,7 +162,9 @@ int d3d_run(d3d_plan plan, void** f1, void** f2, const void* coeff, int count,
  * copies host_f1 to dev_f1, runs `count` steps between dev_f1 and dev_f2,
  * copies the result back into host_f1 and synchronises.  *kernel_ms (may be
  * NULL) receives the device time of the step loop alone (the reference's
- * "Kernel-only performance", :373-384). */
+ * "Kernel-only performance", :373-384); the loop's CUDA graph, captured on
+ * the first call for a given (buffers, count), is built before that timing
+ * starts. */
 int d3d_run_host(d3d_plan plan, void* host_f1, void* dev_f1, void* dev_f2,
                  const void* coeff, int count, void* stream, float* kernel_ms);
 
