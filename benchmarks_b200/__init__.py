@@ -23,7 +23,7 @@ HEADER = os.path.join(ROOT, "include", "d3d_b200.h")
 
 D3D_OK = 0
 D3D_E_INVALID, D3D_E_CUDA, D3D_E_OOM = -1, -2, -3
-D3D_E_TIMEOUT, D3D_E_UNSUPPORTED, D3D_E_BUSY = -4, -5, -6
+D3D_E_TIMEOUT, D3D_E_UNSUPPORTED, D3D_E_BUSY, D3D_E_IO = -4, -5, -6, -7
 F32, F64 = 0, 1
 KERNEL_AUTO, KERNEL_GENERIC, KERNEL_TMA, KERNEL_TB = 0, 1, 2, 3
 NUM_TILE_VARIANTS = 6
@@ -62,6 +62,12 @@ _SIGNATURES = {
     "d3d_analytic": ([_vp, _vp, ctypes.c_double, _vp], _i),
     "d3d_compare": ([_vp, _vp, _i, _vp, _i, _sz, _dp, _vp], _i),
     "d3d_compare_noalloc": ([_vp, _i, _vp, _i, _sz, _dp, _vp], _i),
+    "d3d_checkpoint_save": ([_vp, _vp, ctypes.c_longlong, ctypes.c_char_p,
+                             _vp], _i),
+    "d3d_checkpoint_load": ([_vp, ctypes.c_char_p, _vp,
+                             ctypes.POINTER(ctypes.c_longlong), _vp], _i),
+    "d3d_checkpoint_save_host": ([_vp, _vp, ctypes.c_longlong,
+                                  ctypes.c_char_p], _i),
     "d3d_batch_coefficients": ([_i, _i, _i, ctypes.c_float,
                                 ctypes.POINTER(ctypes.c_float)], _i),
     "d3d_batch_layout": ([_vp, _i, ctypes.POINTER(ctypes.c_size_t)], _i),
@@ -311,6 +317,22 @@ class Plan:
                                  _stream_handle(stream)))
         return out
 
+    def save_checkpoint(self, field, path, step=0, stream=None):
+        """Binary checkpoint of a device field (d3d_checkpoint_save)."""
+        self._check_buf(field)
+        check(lib().d3d_checkpoint_save(self._h, field.data_ptr(), int(step),
+                                        os.fsencode(path),
+                                        _stream_handle(stream)))
+
+    def load_checkpoint(self, path, field, stream=None):
+        """Reads a checkpoint into a device field; returns its step."""
+        self._check_buf(field)
+        step = ctypes.c_longlong()
+        check(lib().d3d_checkpoint_load(self._h, os.fsencode(path),
+                                        field.data_ptr(), ctypes.byref(step),
+                                        _stream_handle(stream)))
+        return step.value
+
     def compare(self, a, b, stream=None):
         """FP64 (rms, max_abs, max_rel, sum(a)) of device field a vs b."""
         import torch
@@ -512,6 +534,67 @@ class Server:
 
 
 NOALLOC_MAX_ELEMENTS = 1 << 28
+
+
+# --- binary checkpoints on the host (the d3d_checkpoint_* file format) ----
+_CKPT_HEADER = np.dtype([("magic", "S8"), ("header_bytes", "<u4"),
+                         ("dtype", "<u4"), ("ndim", "<u4"), ("nx", "<i4"),
+                         ("ny", "<i4"), ("nz", "<i4"), ("step", "<i8"),
+                         ("checksum", "<u8"), ("payload", "<u8"),
+                         ("flags", "<u4"), ("reserved", "<u4")])
+assert _CKPT_HEADER.itemsize == 64
+
+
+def _word_sum(a):
+    """The checksum: the sum of the 32-bit words modulo 2^64."""
+    return int(np.ascontiguousarray(a).view(np.uint32).sum(dtype=np.uint64))
+
+
+def read_checkpoint(path):
+    """(header dict, field array) of a checkpoint file, on the host; the
+    field is (ny, nx) in 2D, (nz, ny, nx) in 3D.  Raises ValueError on a bad
+    magic, size or checksum."""
+    with open(path, "rb") as f:
+        raw = f.read(64)
+        if len(raw) != 64:
+            raise ValueError("%s: truncated header" % path)
+        h = np.frombuffer(raw, _CKPT_HEADER)[0]
+        if h["magic"] != b"D3DCKPT1" or h["header_bytes"] != 64:
+            raise ValueError("%s is not a d3d checkpoint" % path)
+        dt = np.float64 if h["dtype"] == F64 else np.float32
+        shape = ((int(h["ny"]), int(h["nx"])) if h["ndim"] == 2 else
+                 (int(h["nz"]), int(h["ny"]), int(h["nx"])))
+        n = int(np.prod(shape))
+        data = np.fromfile(f, dtype=dt, count=n)
+    if data.size != n or data.nbytes != int(h["payload"]):
+        raise ValueError("%s is truncated" % path)
+    if _word_sum(data) != int(h["checksum"]):
+        raise ValueError("%s failed its checksum" % path)
+    head = {k: (h[k].item() if k != "magic" else h[k].decode())
+            for k in _CKPT_HEADER.names}
+    return head, data.reshape(shape)
+
+
+def write_checkpoint(path, field, step=0, diffusion_surface=False):
+    """Writes a host array as a checkpoint that d3d_checkpoint_load accepts
+    ((ny, nx) arrays are 2D, (nz, ny, nx) arrays 3D)."""
+    a = np.ascontiguousarray(field)
+    if a.dtype not in (np.float32, np.float64) or a.ndim not in (2, 3):
+        raise ValueError("FP32/FP64 2D or 3D array expected")
+    h = np.zeros((), _CKPT_HEADER)
+    h["magic"] = b"D3DCKPT1"
+    h["header_bytes"] = 64
+    h["dtype"] = F64 if a.dtype == np.float64 else F32
+    h["ndim"] = a.ndim
+    h["nx"], h["ny"] = a.shape[-1], a.shape[-2]
+    h["nz"] = a.shape[0] if a.ndim == 3 else 1
+    h["step"] = step
+    h["checksum"] = _word_sum(a)
+    h["payload"] = a.nbytes
+    h["flags"] = 1 if diffusion_surface else 0
+    with open(path, "wb") as f:
+        f.write(h.tobytes())
+        a.tofile(f)
 
 
 def compare_noalloc(a, b, stream=None):

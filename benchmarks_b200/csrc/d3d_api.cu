@@ -732,6 +732,52 @@ int d3d_compare(d3d_plan p, const void* a, int a_dtype, const void* b,
   return D3D_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+d3d::PlanShape shape_of(d3d_plan p) {
+  return d3d::PlanShape{p->nx, p->ny, p->nz, p->ndim, p->flip_y, p->dtype,
+                        p->n};
+}
+
+int ensure_scratch(d3d_plan p) {
+  if (!p->cmp_scratch)
+    D3D_TRY(cudaMalloc(&p->cmp_scratch, d3d::compare_scratch_bytes()),
+            "cudaMalloc (compare scratch)");
+  return D3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int d3d_checkpoint_save(d3d_plan p, const void* field, long long step,
+                        const char* path, void* stream) {
+  if (!p || !field || !path) return fail(D3D_E_INVALID, "NULL argument");
+  int rc = check_device(p);
+  if (!rc) rc = ensure_scratch(p);
+  if (rc) return rc;
+  return d3d::checkpoint_save(shape_of(p), p->cmp_scratch, field, step, path,
+                              as_stream(stream));
+}
+
+int d3d_checkpoint_load(d3d_plan p, const char* path, void* field,
+                        long long* step, void* stream) {
+  if (!p || !field || !path) return fail(D3D_E_INVALID, "NULL argument");
+  int rc = check_device(p);
+  if (!rc) rc = ensure_scratch(p);
+  if (rc) return rc;
+  return d3d::checkpoint_load(shape_of(p), p->cmp_scratch, path, field, step,
+                              as_stream(stream));
+}
+
+int d3d_checkpoint_save_host(d3d_plan p, const void* host_field,
+                             long long step, const char* path) {
+  if (!p || !host_field || !path) return fail(D3D_E_INVALID, "NULL argument");
+  return d3d::checkpoint_save_host(shape_of(p), host_field, step, path);
+}
+
 int d3d_compare_noalloc(const void* a, int a_dtype, const void* b,
                         int b_dtype, size_t n, double out[4], void* stream) {
   if (!a || !b || !out) return fail(D3D_E_INVALID, "NULL argument");

@@ -136,6 +136,20 @@ cudaError_t launch_accuracy(const void* f, int dtype, int ndim, int nx,
                             double time, double* scratch,
                             cudaStream_t stream);
 
+// What the checkpoint code needs of a plan.
+struct PlanShape {
+  int nx, ny, nz, ndim, flip_y, dtype;
+  size_t n;
+};
+// Binary checkpoints (d3d_io.cu).  `scratch` is compare_scratch_bytes() of
+// device memory; the device forms synchronise `s`.
+int checkpoint_save(const PlanShape& ps, double* scratch, const void* field,
+                    long long step, const char* path, cudaStream_t s);
+int checkpoint_load(const PlanShape& ps, double* scratch, const char* path,
+                    void* field, long long* step, cudaStream_t s);
+int checkpoint_save_host(const PlanShape& ps, const void* host_field,
+                         long long step, const char* path);
+
 // A one-CTA kernel whose bounded mbarrier wait is bound to run out.
 cudaError_t launch_selftest_wait(unsigned limit, unsigned* dev_err,
                                  cudaStream_t stream);

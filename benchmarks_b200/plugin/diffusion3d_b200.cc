@@ -49,6 +49,19 @@ void Diffusion3DB200::RunKernel(int count) {
   Check(d3d_run_host(plan_, f1_, f1_d_, f2_d_, coeff, count, nullptr,
                      &kernel_ms_),
         "d3d_run_host");
+  steps_done_ = count;
+}
+
+// The reference's text dump (Baseline::Dump), or with binary_dump the
+// checkpoint of host f1_ beside it: <dump path without ".out">.d3d.
+void Diffusion3DB200::Dump() const {
+  if (!binary_dump_) return Baseline::Dump();
+  std::string path = GetDumpPath();
+  if (path.size() > 4 && path.compare(path.size() - 4, 4, ".out") == 0)
+    path.resize(path.size() - 4);
+  path += ".d3d";
+  Check(d3d_checkpoint_save_host(plan_, f1_, steps_done_, path.c_str()),
+        "d3d_checkpoint_save_host");
 }
 
 void Diffusion3DB200::FinalizeBenchmark() {

@@ -26,19 +26,24 @@ namespace diffusion3d {
 class Diffusion3DB200 : public Baseline {
  public:
   // kernel: D3D_KERNEL_* (AUTO = TMA z-march where eligible); tb_depth: the
-  // fused step count for D3D_KERNEL_TB.
+  // fused step count for D3D_KERNEL_TB; binary_dump: Dump writes a binary
+  // checkpoint (d3d_checkpoint_save_host) instead of the "%.7E" text.
   Diffusion3DB200(int nx, int ny, int nz, int kernel = D3D_KERNEL_AUTO,
-                  int tb_depth = 1)
-      : Baseline(nx, ny, nz), kernel_(kernel), tb_depth_(tb_depth) {}
+                  int tb_depth = 1, bool binary_dump = false)
+      : Baseline(nx, ny, nz), kernel_(kernel), tb_depth_(tb_depth),
+        binary_dump_(binary_dump) {}
   virtual ~Diffusion3DB200() {}
   virtual std::string GetName() const;
   virtual void InitializeBenchmark();
   virtual void RunKernel(int count);
   virtual void FinalizeBenchmark();
   virtual void DisplayResult(int count, float time);
+  virtual void Dump() const;
 
  protected:
   int kernel_, tb_depth_;
+  bool binary_dump_;
+  int steps_done_ = 0;
   d3d_plan plan_ = nullptr;
   void* f1_d_ = nullptr;
   void* f2_d_ = nullptr;

@@ -28,10 +28,12 @@ class DiffusionB200 : public Baseline {
  public:
   // kernel: D3D_KERNEL_* (AUTO: the 2D register march in 2D, the TMA
   // z-march where eligible in 3D); tb_depth: fused steps for D3D_KERNEL_TB
-  // (3D only).
+  // (3D only); binary_dump: Dump writes a binary checkpoint
+  // (d3d_checkpoint_save_host) instead of the "%.7E" text.
   DiffusionB200(int nd, const int* dims, int kernel = D3D_KERNEL_AUTO,
-                int tb_depth = 1)
-      : Baseline(nd, dims), kernel_(kernel), tb_depth_(tb_depth) {}
+                int tb_depth = 1, bool binary_dump = false)
+      : Baseline(nd, dims), kernel_(kernel), tb_depth_(tb_depth),
+        binary_dump_(binary_dump) {}
   virtual ~DiffusionB200() {}
   virtual std::string GetName() const;
   virtual std::string GetDescription() const;
@@ -40,9 +42,12 @@ class DiffusionB200 : public Baseline {
   virtual void RunKernel(int count);
   virtual void FinalizeBenchmark();
   virtual void DisplayResult(int count, float time);
+  virtual void Dump() const;
 
  protected:
   int kernel_, tb_depth_;
+  bool binary_dump_;
+  int steps_done_ = 0;
   d3d_plan plan_ = nullptr;
   void* f1_d_ = nullptr;
   void* f2_d_ = nullptr;

@@ -37,7 +37,9 @@ enum {
   D3D_E_OOM = -3,         /* device or pinned allocation failed */
   D3D_E_TIMEOUT = -4,     /* a bounded device wait ran out */
   D3D_E_UNSUPPORTED = -5, /* shape/dtype/kernel combination not supported */
-  D3D_E_BUSY = -6         /* admission refused (serving) */
+  D3D_E_BUSY = -6,        /* admission refused (serving) */
+  D3D_E_IO = -7           /* a checkpoint file could not be written or read,
+                             or failed its checksum */
 };
 
 enum { D3D_F32 = 0, D3D_F64 = 1 };
@@ -95,7 +97,7 @@ int d3d_diffusion_coefficients(int nd, const int* dims, int dtype,
                                void* coeff7, void* geom8);
 
 /* A plan for a diffusion::Diffusion grid: the launch state
- * DiffusionCUDA keeps (diffusion_cuda.h:44-59).  Every d3d_plan entry point
+ * DiffusionCUDA keeps (diffusion_cuda.h:30-61).  Every d3d_plan entry point
  * below works on it (step, run, run_host, autotune, analytic, compare,
  * accuracy).  nd = 3 runs the 3D kernels in this surface's order and takes
  * any kernel; nd = 2 runs the 2D register-march kernel and takes
@@ -105,8 +107,8 @@ int d3d_diffusion_plan_create(int nd, const int* dims, int dtype, int kernel,
 
 /* Overrides the tile variant (0..D3D_NUM_TILE_VARIANTS-1) and z-chunk
  * (planes per CTA, 0 = automatic) of a plan; used by the autotuner.  On a
- * 2D plan the variant picks the 2D kernel's register-ring depth and L2
- * prefetch distance, and zchunk is the rows per warp task. */
+ * 2D plan the variant picks the 2D kernel's register-ring depth and zchunk
+ * is the rows per warp task. */
 #define D3D_NUM_TILE_VARIANTS 6
 int d3d_plan_set_tile(d3d_plan plan, int variant, int zchunk);
 
@@ -172,6 +174,25 @@ int d3d_run_host(d3d_plan plan, void* host_f1, void* dev_f1, void* dev_f2,
  * with Initialize, diffusion3d.cc:14-39) written to a device buffer of the
  * plan dtype, evaluated in double precision on the device. */
 int d3d_analytic(d3d_plan plan, void* out, double time, void* stream);
+
+/* Binary checkpoints of a field of the plan's shape and dtype: the
+ * replacement for the reference's text dump (Baseline::Dump,
+ * baseline.cc:62-70, one "%.7E" line per value).  The file is a 64-byte
+ * header (magic "D3DCKPT1", dtype, ndim, nx, ny, nz, `step`, the sum of the
+ * payload's 32-bit words modulo 2^64, payload bytes, surface flag) and the
+ * raw field, x fastest (benchmarks_b200.read_checkpoint reads one on a
+ * host).  Device copies go through pinned staging that overlaps PCIe and
+ * file I/O.  Load checks the shape and dtype against the plan
+ * (D3D_E_INVALID) and the stored checksum against the loaded field
+ * (D3D_E_IO); *step (may be NULL) receives the saved step.  The device
+ * forms synchronise `stream`; d3d_checkpoint_save_host writes the same file
+ * from a field in host memory (what a plugin's Dump holds in f1_). */
+int d3d_checkpoint_save(d3d_plan plan, const void* field, long long step,
+                        const char* path, void* stream);
+int d3d_checkpoint_load(d3d_plan plan, const char* path, void* field,
+                        long long* step, void* stream);
+int d3d_checkpoint_save_host(d3d_plan plan, const void* host_field,
+                             long long step, const char* path);
 
 /* Error norms of device field a against device field b (n elements, any
  * dtype pair), accumulated in double on the device: out[0] = rms(a-b),

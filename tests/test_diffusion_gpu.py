@@ -134,8 +134,8 @@ def test_2d_row_chunks(ychunk):
 @pytest.mark.parametrize("ychunk", [0, 3, 16])
 @pytest.mark.parametrize("offset", [0, 1])
 def test_2d_variants(variant, ychunk, offset):
-    """Every ring depth / L2 prefetch variant of the 2D kernel, with 16- and
-    4-byte lanes, against the oracle."""
+    """Every register-ring variant of the 2D kernel, with 16-byte and scalar
+    lanes, against the oracle."""
     ny, nx = 150, 1028
     c, _ = O.dif_params(2, nx, ny)
     f = O.dif_initialize(2, nx, ny) + O.seeded_noise((ny, nx), 6)

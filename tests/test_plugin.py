@@ -147,3 +147,15 @@ def test_driver_dump_matches_oracle(tmp_path):
     c, _ = O.params(24, 24, 24)
     ref = O.run(O.initialize(24, 24, 24), c, 13)
     assert lines == ["%.7E" % v for v in ref.reshape(-1).astype(np.float64)]
+
+
+@pytest.mark.gpu
+def test_driver_binary_dump_matches_oracle(tmp_path):
+    import benchmarks_b200 as B
+    _run_driver(STANDALONE, "--size", "24", "--count", "13", "--dump-binary",
+                cwd=str(tmp_path))
+    h, field = B.read_checkpoint(str(tmp_path / "diffusion3d_result.b200.d3d"))
+    c, _ = O.params(24, 24, 24)
+    ref = O.run(O.initialize(24, 24, 24), c, 13)
+    assert field.tobytes() == ref.tobytes()
+    assert h["step"] == 13 and h["flags"] == 0

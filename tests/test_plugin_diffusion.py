@@ -183,3 +183,15 @@ def test_driver_dump_matches_oracle(tmp_path):
     c, _ = O.dif_params(2, 40, 40)
     ref = O.dif_run(O.dif_initialize(2, 40, 40), c, 13)
     assert lines == ["%.7E" % v for v in ref.reshape(-1).astype(np.float64)]
+
+
+@pytest.mark.gpu
+def test_driver_binary_dump_matches_oracle(tmp_path):
+    import benchmarks_b200 as B
+    _run_driver(STANDALONE, "--nd", "2", "--size", "40", "--count", "13",
+                "--dump-binary", cwd=str(tmp_path))
+    h, field = B.read_checkpoint(str(tmp_path / "diffusion_result.b200.d3d"))
+    c, _ = O.dif_params(2, 40, 40)
+    ref = O.dif_run(O.dif_initialize(2, 40, 40), c, 13)
+    assert field.tobytes() == ref.tobytes()
+    assert h["step"] == 13 and h["flags"] == 1 and h["ndim"] == 2
