@@ -258,6 +258,20 @@ __device__ __forceinline__ void tma_load_3d(void* smem_dst,
       : "memory");
 }
 
+// `fallback`, or the shared-memory word at p where `pred` holds: a
+// predicated load with no branch around it.
+__device__ __forceinline__ float ld_shared_if(bool pred, const float* p,
+                                              float fallback) {
+  float r = fallback;
+  asm volatile(
+      "{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %1, 0;\n\t"
+      "@q ld.shared.f32 %0, [%2];\n\t}"
+      : "+f"(r)
+      : "r"((int)pred), "r"(smem_u32(p))
+      : "memory");
+  return r;
+}
+
 __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap* map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(
                    reinterpret_cast<uint64_t>(map))

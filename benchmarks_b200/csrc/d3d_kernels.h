@@ -90,6 +90,16 @@ int tb_box_x(int dtype, int k);
 int tb_box_y(int k);
 bool tb_supported(int k, int dtype);
 
+// Two fused steps, FP32, warp-row tiles (d3d_tb2.cu): the default TB
+// kernel for K = 2 in FP32; the generic-K kernel stays selectable.
+cudaError_t launch_steps_tb2w(const CUtensorMap& src, void* f2, int nx,
+                              int ny, int nz, const void* coef,
+                              int zchunk_override, int flip_y,
+                              cudaStream_t stream, unsigned* dev_err,
+                              LaunchInfo* info);
+int tb2w_box_x();
+int tb2w_box_y();
+
 // FP64-accumulated comparison of two device fields (any dtype pair):
 // out[0] = rms(a-b), out[1] = max|a-b|, out[2] = max|a-b|/|b|, out[3] = sum(a).
 // `scratch` holds `compare_scratch_bytes()` bytes of device memory.

@@ -176,7 +176,8 @@ __global__ void __launch_bounds__(TbCfg<T, K, BY, S0>::THREADS,
   V16<T> X[3][C::KM1][NI];
 
   int drain_lo = lo0, drain_hi = min(hi0, lo0 + S0 - 1);
-  bool ok = mbar_wait_bounded(&bars[stage_of(lo0)], parity_of(lo0));
+  // Thread 0 makes every mbarrier wait; the CTA barrier releases the rest.
+  bool ok = tid != 0 || mbar_wait_bounded(&bars[stage_of(lo0)], parity_of(lo0));
   int qf = -1;  // iteration whose wait ran out
   if (!__syncthreads_and(ok)) {
     if (tid == 0) atomicOr(dev_err, kDevWaitTimeout);
@@ -239,7 +240,7 @@ __global__ void __launch_bounds__(TbCfg<T, K, BY, S0>::THREADS,
         }
       // Level 1 of the next iteration reads level-0 planes q-1..q+1.
       bool ok2 = true;
-      if (q + 1 <= hi0)
+      if (tid == 0 && q + 1 <= hi0)
         ok2 = mbar_wait_bounded(&bars[stage_of(q + 1)], parity_of(q + 1));
       if (!__syncthreads_and(ok2)) {
         if (tid == 0) atomicOr(dev_err, kDevWaitTimeout);

@@ -45,7 +45,10 @@ enum {
 enum { D3D_F32 = 0, D3D_F64 = 1 };
 
 enum {
-  D3D_KERNEL_AUTO = 0,    /* TMA z-march when eligible, else generic */
+  D3D_KERNEL_AUTO = 0,    /* TMA z-march when eligible, else generic;
+                             FP32 3D grids of 2^27+ points run pairs of
+                             steps as fused two-step passes (faster there
+                             on B200, same bits) */
   D3D_KERNEL_GENERIC = 1, /* any shape / alignment */
   D3D_KERNEL_TMA = 2,     /* TMA-staged z-march (row pitch % 16 B == 0) */
   D3D_KERNEL_TB = 3       /* temporal blocking: tb_depth fused steps/pass */

@@ -148,6 +148,43 @@ def test_temporal_blocking_short_chunks(k, zchunk):
         assert bits_equal(out, O.run(fin, c, count)), count
 
 
+@pytest.mark.parametrize("dims", [(128, 14, 7), (132, 30, 9), (260, 29, 33),
+                                  (256, 64, 40), (64, 1, 1), (128, 15, 2),
+                                  (136, 17, 3), (4, 3, 5)])
+@pytest.mark.parametrize("zchunk", [0, 1, 2, 5])
+def test_tb2_warp_row_kernel_vs_generic_and_oracle(dims, zchunk):
+    """The K = 2 FP32 warp-row kernel (TB variant 0) against the generic-K
+    kernel (variant 1) and the oracle: tiles of 128 x 14 cut by every edge
+    case (nx not a multiple of 128, ny not a multiple of 14, nz of 1..3,
+    one-plane z-chunks), even and odd step counts."""
+    nx, ny, nz = dims
+    c, _ = O.params(nx, ny, nz)
+    fin = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), 21)
+    for count in (2, 5):
+        ref = O.run(fin, c, count)
+        outs = []
+        for variant in (0, 1):
+            out = gpu_run(fin, c, count, B.KERNEL_TB, 2, variant=variant,
+                          zchunk=zchunk)
+            outs.append(out)
+        assert bits_equal(outs[0], ref), (dims, zchunk, count)
+        assert bits_equal(outs[1], ref), (dims, zchunk, count)
+
+
+def test_tb2_warp_row_kernel_is_the_default():
+    plan = B.Plan(128, 28, 8, B.F32, B.KERNEL_TB, 2)
+    f1, f2 = plan.empty(), plan.empty()
+    f1.uniform_()
+    plan.run(f1, f2, 2)
+    torch.cuda.synchronize()
+    assert plan.info()["last_kernel"] == "steps_tb2w"
+    plan.set_tile(1, 0)
+    plan.run(f1, f2, 2)
+    torch.cuda.synchronize()
+    assert plan.info()["last_kernel"] == "steps_tb"
+    plan.close()
+
+
 def test_tma_rejects_ineligible_and_auto_falls_to_generic():
     nx, ny, nz = 17, 8, 4  # row pitch 68 B: not a multiple of 16
     plan = B.Plan(nx, ny, nz, B.F32, B.KERNEL_TMA)
