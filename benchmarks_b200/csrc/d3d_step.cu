@@ -77,8 +77,9 @@ __global__ void __launch_bounds__(StepTmaCfg<T, BY, S>::THREADS)
   const int pbase = z0 > 0 ? z0 - 1 : 0;  // first plane loaded (b of z0)
   const int plast = min(z1, nz - 1);      // last plane needed (t of z1-1)
 
-  auto stage_of = [&](int p) { return (p - pbase) % S; };
-  auto parity_of = [&](int p) { return (unsigned)(((p - pbase) / S) & 1); };
+  // p >= pbase always: unsigned arithmetic keeps these a mask and a shift.
+  auto stage_of = [&](int p) { return (int)((unsigned)(p - pbase) % S); };
+  auto parity_of = [&](int p) { return ((unsigned)(p - pbase) / S) & 1u; };
   auto stage_ptr = [&](int p) { return stages + stage_of(p) * C::STAGE_ELEMS; };
   auto issue = [&](int p) {
     const int s = stage_of(p);

@@ -11,7 +11,7 @@
 //            rows x a z-chunk; level 1 covers 16 rows (one halo row above
 //            and below) and, through two scalar halo columns, x0-1 and
 //            x0+128; level 0 is TMA-loaded as 136 x 18 boxes (x0-4 ..
-//            x0+131, y0-2 .. y0+15) into a 5-plane shared ring (mbarriers);
+//            x0+131, y0-2 .. y0+15) into a 4-plane shared ring (mbarriers);
 //   warps    warp w owns level-1 rows 2w and 2w+1 of the 16 and the same
 //            rows at level 2 (rows 1..14 only): warps 0 and 7 have one
 //            level-2 row, and they compute the left and right level-1 halo
@@ -53,7 +53,10 @@ struct Tb2w {
   static constexpr int BY = R1 - 2;             // 14 output rows
   static constexpr int R0 = R1 + 2;             // 18 level-0 rows
   static constexpr int RPW = R1 / WARPS;        // 2 rows per warp
-  static constexpr int S0 = 5;                  // level-0 ring planes
+  // Level-0 ring planes: q-2, q-1, q in use and one load in flight, which
+  // is a whole iteration (about 3.5 us at 512^3) ahead of its use; a power
+  // of two keeps the stage and parity arithmetic to a mask and a shift.
+  static constexpr int S0 = 4;
   static constexpr int STAGE_RAW = P * R0 * 4;  // 9792 bytes
   static constexpr int STAGE = (STAGE_RAW + 127) / 128 * 128;
   static constexpr int STAGE_ELEMS = STAGE / 4;
@@ -90,8 +93,9 @@ __global__ void __launch_bounds__(Tb2w::THREADS, MINB)
   const int lo1 = max(z0 - 1, 0), hi1 = min(z1, nz - 1);
   const int lo0 = max(z0 - 2, 0), hi0 = min(z1 + 1, nz - 1);
 
-  auto stage_of = [&](int p) { return (p - lo0) % S0; };
-  auto parity_of = [&](int p) { return (unsigned)(((p - lo0) / S0) & 1); };
+  // p >= lo0 always: unsigned arithmetic makes these a mask and a shift.
+  auto stage_of = [&](int p) { return (int)((unsigned)(p - lo0) % S0); };
+  auto parity_of = [&](int p) { return ((unsigned)(p - lo0) / S0) & 1u; };
   auto stage_ptr = [&](int p) {
     return stages + stage_of(p) * C::STAGE_ELEMS;
   };
@@ -318,10 +322,10 @@ cudaError_t launch_tb2w_t(const CUtensorMap& src, void* f2, int nx, int ny,
   (void)sms;
   int zchunk = zchunk_override;
   if (zchunk <= 0) {
-    // Measured on B200 (Gpt-updates/s): 96-plane chunks at 512^3 (837) and
-    // 768^3 (849); below 512 planes, 32-plane chunks keep enough CTAs in
-    // flight (384^3: 747 against 572-683 for 48-128).
-    zchunk = std::min(nz, nz >= 512 ? 96 : 32);
+    // Measured on B200 (Gpt-updates/s): 96-plane chunks at 512^3 (826-837)
+    // and 768^3 (849); shorter grids need more chunks to keep CTAs in
+    // flight (384^3: 32 planes, 743 against 573-695 for 48-128; 256^3: 16).
+    zchunk = std::min(nz, nz >= 512 ? 96 : nz >= 384 ? 32 : 16);
   }
   const int gz = (nz + zchunk - 1) / zchunk;
   if (info) *info = LaunchInfo{gx, gy, gz, C::THREADS, C::SMEM, zchunk, occ};
