@@ -231,27 +231,34 @@ def serving_leg(B, torch, n_req=96, arena_gb=24.0, chunk=8):
             np.percentile(lat, 99)), "makespan_s": span,
             "value": upd / span / 1e9}
 
-    # served
-    server = B.Server(int(arena_gb * 2 ** 30), chunk)
-    done_at = [0.0] * n_req
-    idmap = {}
-    nxt = 0
-    t0 = time.perf_counter()
-    while len(idmap) < n_req or sum(server.pending()):
-        now = time.perf_counter() - t0
-        while nxt < n_req and reqs[nxt][0] <= now:
-            _, s, st = reqs[nxt]
-            hin = pool_in[:s ** 3].reshape(s, s, s)
-            hout = out_pool[offs[nxt]:offs[nxt] + s ** 3].reshape(s, s, s)
-            idmap[server.submit(hin, hout, st, coeff[s])] = nxt
-            nxt += 1
-        for rid in server.tick():
-            done_at[idmap[rid]] = time.perf_counter() - t0
-        if nxt < n_req and not sum(server.pending()):
-            time.sleep(max(0.0, reqs[nxt][0] - (time.perf_counter() - t0)))
-    served = lat_stats(done_at)
-    served["stats"] = server.stats()
-    server.close()
+    def serve(kernel=None, lanes=None):
+        server = B.Server(int(arena_gb * 2 ** 30), chunk, kernel, lanes)
+        done_at = [0.0] * n_req
+        idmap = {}
+        nxt = 0
+        t0 = time.perf_counter()
+        while len(idmap) < n_req or sum(server.pending()):
+            now = time.perf_counter() - t0
+            while nxt < n_req and reqs[nxt][0] <= now:
+                _, s, st = reqs[nxt]
+                hin = pool_in[:s ** 3].reshape(s, s, s)
+                hout = out_pool[offs[nxt]:offs[nxt] + s ** 3].reshape(s, s, s)
+                idmap[server.submit(hin, hout, st, coeff[s])] = nxt
+                nxt += 1
+            for rid in server.tick():
+                done_at[idmap[rid]] = time.perf_counter() - t0
+            if nxt < n_req and not sum(server.pending()):
+                time.sleep(max(0.0, reqs[nxt][0] - (time.perf_counter() - t0)))
+        out = lat_stats(done_at)
+        out["stats"] = server.stats()
+        server.close()
+        return out
+
+    # served: the default server (pitched TMA step kernel, several
+    # streams), then the same stream through the batch API's march kernel
+    # on one stream for comparison
+    served = serve()
+    march = serve(kernel=-1, lanes=1)
     # plain per-request loop
     import ctypes
     done_at = [0.0] * n_req
@@ -278,7 +285,10 @@ def serving_leg(B, torch, n_req=96, arena_gb=24.0, chunk=8):
         done_at[i] = time.perf_counter() - t0
     plain = lat_stats(done_at)
     return {"requests": n_req, "rate_per_s": 2000.0, "updates": upd,
-            "unit": UNIT, "served": served, "plain_loop": plain,
+            "unit": UNIT, "served": served,
+            "served_march_one_stream": {
+                k: march[k] for k in ("solves_per_s", "makespan_s", "value")},
+            "plain_loop": plain,
             "speedup_solves": served["solves_per_s"] / plain["solves_per_s"],
             "p99_ratio_plain_over_served": plain["p99_ms"] / served["p99_ms"]}
 

@@ -86,6 +86,8 @@ _SIGNATURES = {
                             ctypes.POINTER(ctypes.c_int),
                             ctypes.POINTER(ctypes.c_int)], _i),
     "d3d_server_stats": ([_vp, ctypes.c_char_p, _sz], _i),
+    "d3d_server_set_kernel": ([_vp, _i], _i),
+    "d3d_server_set_lanes": ([_vp, _i], _i),
     "d3d_server_destroy": ([_vp], _i),
     "d3d_check_device_errors": ([ctypes.POINTER(ctypes.c_uint)], _i),
     "d3d_accuracy": ([_vp, _vp, _i, _dp, _vp], _i),
@@ -471,11 +473,15 @@ class Server:
     asynchronous copies); tick() runs one scheduling round and returns the
     ids that finished."""
 
-    def __init__(self, arena_bytes, chunk=8):
+    def __init__(self, arena_bytes, chunk=8, kernel=None, lanes=None):
         h = ctypes.c_void_p()
         check(lib().d3d_server_create(int(arena_bytes), chunk,
                                       ctypes.byref(h)))
         self._h = h
+        if kernel is not None:
+            self.set_kernel(kernel)
+        if lanes is not None:
+            self.set_lanes(lanes)
         self._keep = {}
         self._ids = (ctypes.c_longlong * 4096)()
 
@@ -501,6 +507,15 @@ class Server:
         for i in done:
             self._keep.pop(i, None)
         return done
+
+    def set_kernel(self, kernel):
+        """Step kernel of the idle server: 0..4 the pitched TMA kernel's
+        tile shapes (3 is the default), -1 the batch API's march kernel."""
+        check(lib().d3d_server_set_kernel(self._h, int(kernel)))
+
+    def set_lanes(self, lanes):
+        """Compute streams of the idle server (1..4, default 4)."""
+        check(lib().d3d_server_set_lanes(self._h, int(lanes)))
 
     def pending(self):
         q, a, r = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

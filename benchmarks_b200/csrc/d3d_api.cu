@@ -136,6 +136,7 @@ int set_cuda_error(cudaError_t e, const char* what) {
 void note_launches(unsigned long long n) {
   g_launches.fetch_add(n, std::memory_order_relaxed);
 }
+unsigned* device_error_word() { return dev_error_ptr(); }
 }  // namespace d3d
 
 struct d3d_plan_s {

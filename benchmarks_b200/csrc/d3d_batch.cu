@@ -12,9 +12,10 @@
 // contributes one work item per xy tile, so the items still active at step
 // s are a prefix of the class's list: step s launches exactly that prefix.
 //
-// Tile kernel: d3d::march_tile (d3d_march.cuh) over all nz planes of the
-// item's grid.  Each point is d3d::point: results are bit-identical to
-// running each grid alone.
+// Tile kernel: d3d::march_tile (d3d_march.cuh) over one z slab of the
+// item's grid (the batch API uses one slab of all nz planes; the solve
+// server cuts large grids into several).  Each point is d3d::point: results
+// are bit-identical to running each grid alone.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -40,17 +41,19 @@ __global__ void __launch_bounds__(256)
   __shared__ __align__(16) float stage[2][TileT::E];
   const int2 it = items[blockIdx.x];
   const BatchDesc d = descs[it.x];
-  const int bx = it.y % d.tiles_x, by = it.y / d.tiles_x;
+  const int txy = it.y % d.tiles_xy, zs = it.y / d.tiles_xy;
+  const int bx = txy % d.tiles_x, by = txy / d.tiles_x;
+  const int z0 = zs * d.zc, z1 = min(d.nz, z0 + d.zc);
   const float* src = parity ? d.b : d.a;
   float* dst = parity ? d.a : d.b;
   const Coef<float> k{d.k[0], d.k[1], d.k[2], d.k[3],
                       d.k[4], d.k[5], d.k[6], d.k[7]};
   if constexpr (PAIR)
-    march_tile2<BX, BY>(src, dst, d.nx, d.ny, d.nz, bx * BX, by * BY, 0,
-                        d.nz, k, stage);
+    march_tile2<BX, BY>(src, dst, d.nx, d.ny, d.nz, bx * BX, by * BY, z0,
+                        z1, k, stage);
   else
     march_tile<float, BX, BY>(src, dst, d.nx, d.ny, d.nz, bx * BX, by * BY,
-                              0, d.nz, k, stage);
+                              z0, z1, k, stage);
 }
 
 // Shape 0 (32 x 16 cells as x-pairs) is the default, the autotuner's pick
@@ -154,6 +157,8 @@ int build_class(d3d_batch b, ClassPlan& c) {
     d.nz = g.nz;
     d.tiles_x = (g.nx + sh.bx - 1) / sh.bx;
     const int tiles = d.tiles_x * ((g.ny + sh.by - 1) / sh.by);
+    d.tiles_xy = tiles;
+    d.zc = g.nz;  // one slab: batches bring parallelism in grid count
     for (int j = 0; j < 7; ++j) d.k[j] = g.coeff[j];
     d.k[7] = -0.0f;
     descs.push_back(d);

@@ -117,13 +117,52 @@ cudaError_t launch_compare_noalloc(const void* a, int a_dtype, const void* b,
                                    cudaStream_t stream);
 
 // One grid of a multi-grid step launch: step `parity` reads a (parity 0)
-// or b (parity 1) and writes the other.
+// or b (parity 1) and writes the other.  A work item (grid, tile) names
+// xy tile `tile % tiles_xy` (x fastest, tiles_x per row) and z slab
+// `tile / tiles_xy` of `zc` planes.
 struct BatchDesc {
   float* a;
   float* b;
   int nx, ny, nz, tiles_x;
+  int tiles_xy, zc;
   float k[8];  // ce, cw, cn, cs, ct, cb, cc, and -0.0
 };
+
+// One grid of a pitched multi-grid TMA launch (the solve server's layout):
+// rows of px >= nx floats (px a multiple of 4), pads x in [nx, px) holding
+// copies of column nx-1; map[0] / map[1] cover a / b as px x ny x nz
+// fields.  Items as for BatchDesc.
+struct alignas(64) PitchedDesc {
+  CUtensorMap map[2];
+  float* a;
+  float* b;
+  int nx, px, ny, nz, tiles_x, tiles_xy, zc, unused;
+  float k[8];  // ce, cw, cn, cs, ct, cb, cc, and -0.0
+};
+
+// Tile shapes of the pitched kernel: `lanes` per tile row (tile width
+// 4 * lanes), `by` rows, `stages` planes in the TMA ring.
+struct PitchedVariant {
+  int lanes, by, stages;
+};
+constexpr int kNumPitchedVariants = 5;
+const PitchedVariant& pitched_variant(int v);
+int pitched_box_x(int v);
+int pitched_box_y(int v);
+
+// One time step for `nitems` (grid, tile) work items of pitched grids.
+cudaError_t launch_pitched_step(int variant, const PitchedDesc* descs,
+                                const int2* items, int nitems, int parity,
+                                cudaStream_t s, unsigned* dev_err);
+
+// Dense rows (nx floats) -> pitched rows (px floats, pads filled from
+// column nx-1) when to_pitched, else pitched -> dense; rows = ny * nz.
+// src and dst must not overlap.
+cudaError_t launch_repitch(const float* src, float* dst, int nx, int px,
+                           long long rows, bool to_pitched, cudaStream_t s);
+
+// This device's kernel error word (bounded-wait failures).
+unsigned* device_error_word();
 
 // Tile shapes of the multi-grid step kernel (256 threads each).
 struct BShape {

@@ -1,0 +1,311 @@
+// Multi-grid TMA step over pitched grids: the solve server's step kernel.
+//
+// The server keeps every solve in its device arena with a row pitch
+// px = nx rounded up to 4 floats (16 bytes), so any grid, whatever its nx,
+// can be read with TMA box loads (a tensor map's row stride must be a
+// multiple of 16 bytes).  The pad columns x in [nx, px) hold copies of
+// column nx-1 -- the replicated x boundary of the reference
+// (diffusion3d_openmp.cc:52-53, `e = (x == nx-1) ? c : c + 1`) stored in
+// memory -- and every step rewrites them from its own output.  The e
+// neighbour of x = nx-1 is then read like any other neighbour and equals
+// the centre value, so results are bit-identical to the unpadded field.
+//
+// Work items are (grid, tile) pairs as in the march kernel (d3d_batch.cu):
+// tile = slab * tiles_xy + xy tile.  Each CTA runs the z-march of the
+// single-grid TMA kernel (d3d_step.cu) on one tile of one z slab: one
+// thread issues a 3-D box load per plane into a ring of S shared stages
+// completed through mbarriers (bounded waits), b/c/t of each thread's
+// 16-byte segments live in registers, x neighbours come from shuffles
+// within the row's lanes, y neighbours from shared memory, and every output
+// segment is one 16-byte store.  A row of the tile is LPR lanes wide
+// (LPR = 32: 128-column tiles; LPR = 16: 64-column tiles, two rows per warp
+// instruction), which bounds the columns wasted on narrow grids.
+//
+// The two tensor maps of each grid (its a and b buffers) sit in the work
+// descriptors in global memory, rewritten by the host between launches; the
+// issuing thread acquires each map through the tensormap proxy before use.
+#include <algorithm>
+#include <cstdio>
+
+#include "d3d_common.cuh"
+#include "d3d_kernels.h"
+
+namespace d3d {
+
+template <int LPR, int BY, int S>
+struct PitchedCfg {
+  static constexpr int WARPS = 8;
+  static constexpr int THREADS = WARPS * 32;
+  static constexpr int V = 4;             // floats per 16-byte segment
+  static constexpr int BX = LPR * V;      // tile width
+  static constexpr int HX = V;            // 16-byte x halo on each side
+  static constexpr int P = BX + 2 * HX;   // shared row pitch (floats)
+  static constexpr int R = BY + 2;        // rows per stage (1-row y halo)
+  static constexpr int SEGR = 32 / LPR;   // rows per warp instruction
+  static constexpr int RPW = BY / WARPS;  // tile rows per warp
+  static constexpr int NR = RPW / SEGR;   // row sets per thread
+  static constexpr int STAGE_BYTES_RAW = P * R * 4;
+  static constexpr int STAGE_BYTES = (STAGE_BYTES_RAW + 127) / 128 * 128;
+  static constexpr int STAGE_ELEMS = STAGE_BYTES / 4;
+  static constexpr int SMEM = S * STAGE_BYTES + S * 8 + 128;
+  static_assert(LPR == 32 || LPR == 16, "a tile row is 16 or 32 lanes");
+  static_assert(BY % WARPS == 0 && RPW % SEGR == 0 && NR >= 1,
+                "every warp owns whole row sets");
+  static_assert(P <= 256 && R <= 256, "TMA box dimensions are at most 256");
+  static_assert(S >= 4, "the ring keeps planes z, z+1, z+2 and one in flight");
+};
+
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(
+                   reinterpret_cast<uint64_t>(map))
+               : "memory");
+}
+
+template <int LPR, int BY, int S>
+__global__ void __launch_bounds__(256)
+    pitched_step_kernel(const PitchedDesc* __restrict__ descs,
+                        const int2* __restrict__ items, int parity,
+                        unsigned* __restrict__ dev_err) {
+  using C = PitchedCfg<LPR, BY, S>;
+  constexpr int V = C::V;
+  constexpr int NR = C::NR;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  float* stages = reinterpret_cast<float*>(base);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + S * C::STAGE_BYTES);
+
+  const int2 it = items[blockIdx.x];
+  const PitchedDesc* dp = descs + it.x;
+  const CUtensorMap* src = &dp->map[parity];
+  float* __restrict__ dst = parity ? dp->a : dp->b;
+  const int nx = dp->nx, px = dp->px, ny = dp->ny, nz = dp->nz;
+  const int txy = it.y % dp->tiles_xy, zs = it.y / dp->tiles_xy;
+  const int x0 = (txy % dp->tiles_x) * C::BX;
+  const int y0 = (txy / dp->tiles_x) * BY;
+  const int z0 = zs * dp->zc;
+  const int z1 = min(nz, z0 + dp->zc);
+  if (z0 >= z1) return;
+  const Coef<float> k{dp->k[0], dp->k[1], dp->k[2], dp->k[3],
+                      dp->k[4], dp->k[5], dp->k[6], dp->k[7]};
+  const int pbase = z0 > 0 ? z0 - 1 : 0;  // first plane loaded (b of z0)
+  const int plast = min(z1, nz - 1);      // last plane needed (t of z1-1)
+
+  auto stage_of = [&](int p) { return (int)((unsigned)(p - pbase) % S); };
+  auto parity_of = [&](int p) { return ((unsigned)(p - pbase) / S) & 1u; };
+  auto stage_ptr = [&](int p) { return stages + stage_of(p) * C::STAGE_ELEMS; };
+  auto issue = [&](int p) {
+    const int s = stage_of(p);
+    mbar_arrive_expect_tx(&bars[s], C::STAGE_BYTES_RAW);
+    tma_load_3d(stages + s * C::STAGE_ELEMS, src, &bars[s], x0 - C::HX,
+                y0 - 1, p);
+  };
+
+  if (threadIdx.x == 0) {
+    tensormap_acquire(src);
+    tma_prefetch_desc(src);
+    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int p = pbase; p <= plast && p < pbase + S; ++p) issue(p);
+  }
+
+  // Addressing.  Boundary rules are addresses, as in the single-grid
+  // kernel: y = 0 / ny-1 read the centre row as n / s, x = 0 reads its own
+  // value as w; x = nx-1 reads the pad (a copy of itself) as e, or, when nx
+  // fills its last segment, takes its own value for the lane's er.
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int sl = lane % LPR, sub = lane / LPR;
+  const int xg = x0 + V * sl;
+  const int col = C::HX + V * sl;
+  const bool x_hi = (xg + V - 1 == nx - 1);
+  // The segment that holds x = nx-1 followed by pads: its pad outputs are
+  // replaced by the value at nx-1 so the pads stay copies of that column.
+  const bool x_cross = (xg < nx) && (xg + V > nx);
+  const int jh = nx - 1 - xg;  // index of x = nx-1 in that segment
+  int c_off[NR], n_off[NR], s_off[NR];
+  size_t g_off[NR];
+  bool store_ok[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    const int row = warp * C::RPW + r * C::SEGR + sub;
+    const int yg = y0 + row;
+    c_off[r] = (row + 1) * C::P + col;
+    n_off[r] = (yg == 0) ? c_off[r] : row * C::P + col;
+    s_off[r] = (yg >= ny - 1) ? c_off[r] : (row + 2) * C::P + col;
+    g_off[r] = (size_t)yg * px + xg;
+    store_ok[r] = (yg < ny) && (xg < px);
+  }
+  const int wl_adj = (xg == 0) ? 0 : -1;
+  const size_t plane = (size_t)px * ny;
+  const Coef2 kk = coef2(k);
+
+  V16<float> q0[NR], q1[NR], q2[NR];
+  int drain_lo = pbase, drain_hi = min(plast, pbase + S - 1);
+
+  bool ok = mbar_wait_bounded(&bars[stage_of(z0)], parity_of(z0));
+  if (z0 > 0) ok = ok && mbar_wait_bounded(&bars[stage_of(z0 - 1)],
+                                           parity_of(z0 - 1));
+  if (z0 + 1 <= plast)
+    ok = ok && mbar_wait_bounded(&bars[stage_of(z0 + 1)], parity_of(z0 + 1));
+  if (!__syncthreads_and(ok)) {
+    if (threadIdx.x == 0) atomicOr(dev_err, kDevWaitTimeout);
+    goto drain;
+  }
+  {
+    const float* sc = stage_ptr(z0);
+    const float* sb = stage_ptr(pbase);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      q1[r] = ld16_shared(sc + c_off[r]);
+      q0[r] = ld16_shared(sb + c_off[r]);
+    }
+  }
+  __syncthreads();
+  if (z0 > 0 && threadIdx.x == 0 && pbase + S <= plast) issue(pbase + S);
+
+  {
+    auto step = [&](int z, const V16<float>* vb, const V16<float>* vc,
+                    V16<float>* vt) -> bool {
+      const float* sc = stage_ptr(z);
+      const float* st = stage_ptr(min(z + 1, nz - 1));
+      float* out = dst + (size_t)z * plane;
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        vt[r] = ld16_shared(st + c_off[r]);
+        const V16<float> n = ld16_shared(sc + n_off[r]);
+        const V16<float> s = ld16_shared(sc + s_off[r]);
+        float wl = __shfl_up_sync(0xffffffffu, vc[r].e[V - 1], 1, LPR);
+        float er = __shfl_down_sync(0xffffffffu, vc[r].e[0], 1, LPR);
+        if (sl == 0) wl = sc[c_off[r] + wl_adj];
+        if (sl == LPR - 1) er = sc[c_off[r] + V];
+        if (x_hi) er = vc[r].e[V - 1];
+        V16<float> o = point_seg<float>(kk, vc[r], n, s, vb[r], vt[r], wl, er);
+        if (x_cross) {
+          if (jh < 1) o.e[1] = o.e[0];
+          if (jh < 2) o.e[2] = o.e[1];
+          o.e[3] = o.e[2];
+        }
+        if (store_ok[r]) st16_global(out + g_off[r], o);
+      }
+      bool ok2 = true;
+      if (z + 2 <= plast && z + 1 < z1)
+        ok2 = mbar_wait_bounded(&bars[stage_of(z + 2)], parity_of(z + 2));
+      if (!__syncthreads_and(ok2)) {
+        if (threadIdx.x == 0) atomicOr(dev_err, kDevWaitTimeout);
+        return false;
+      }
+      if (threadIdx.x == 0 && z + S <= plast) issue(z + S);
+      return true;
+    };
+
+    int zf = -1;
+    for (int z = z0; z < z1; z += 3) {
+      if (!step(z, q0, q1, q2)) { zf = z; break; }
+      if (z + 1 >= z1) break;
+      if (!step(z + 1, q1, q2, q0)) { zf = z + 1; break; }
+      if (z + 2 >= z1) break;
+      if (!step(z + 2, q2, q0, q1)) { zf = z + 2; break; }
+    }
+    if (zf >= 0) {
+      drain_lo = zf + 2;
+      drain_hi = min(plast, zf + S - 1);
+      goto drain;
+    }
+  }
+  return;
+
+drain:
+  // A wait ran out: let every load issued and not yet waited for land
+  // before the CTA's shared memory is released.  Bounded as well.
+  if (threadIdx.x == 0) {
+    for (int p = drain_lo; p <= drain_hi; ++p) {
+      bool done = false;
+      for (unsigned i = 0; i < (kMaxWaitIters >> 4) && !done; ++i)
+        done = mbar_try_wait(&bars[stage_of(p)], parity_of(p));
+      if (!done) {
+        atomicOr(dev_err, kDevDrainTimeout);
+        break;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Between the host's dense rows (nx floats) and the arena's pitched rows
+// (px floats): `to_pitched` writes every x in [0, px) of dst from
+// src[min(x, nx-1)], which also fills the pads; otherwise dst takes the
+// first nx floats of each pitched row.  Blocks stride over rows.
+__global__ void __launch_bounds__(128)
+    repitch_kernel(const float* __restrict__ src, float* __restrict__ dst,
+                   int nx, int px, long long rows, bool to_pitched) {
+  for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+    if (to_pitched) {
+      const float* in = src + (size_t)r * nx;
+      float* out = dst + (size_t)r * px;
+      for (int x = threadIdx.x; x < px; x += blockDim.x)
+        out[x] = in[min(x, nx - 1)];
+    } else {
+      const float* in = src + (size_t)r * px;
+      float* out = dst + (size_t)r * nx;
+      for (int x = threadIdx.x; x < nx; x += blockDim.x) out[x] = in[x];
+    }
+  }
+}
+
+namespace {
+
+// (row lanes, rows per tile, planes in the ring).
+const PitchedVariant kPitched[kNumPitchedVariants] = {
+    {16, 16, 4}, {32, 16, 4}, {32, 32, 4}, {16, 32, 4}, {32, 8, 4}};
+
+template <int LPR, int BY, int S>
+cudaError_t launch_t(const PitchedDesc* descs, const int2* items, int n,
+                     int parity, cudaStream_t s, unsigned* dev_err) {
+  using C = PitchedCfg<LPR, BY, S>;
+  auto kern = pitched_step_kernel<LPR, BY, S>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(
+        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  kern<<<n, C::THREADS, C::SMEM, s>>>(descs, items, parity, dev_err);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+const PitchedVariant& pitched_variant(int v) { return kPitched[v]; }
+
+int pitched_box_x(int v) { return kPitched[v].lanes * 4 + 8; }
+int pitched_box_y(int v) { return kPitched[v].by + 2; }
+
+cudaError_t launch_pitched_step(int variant, const PitchedDesc* descs,
+                                const int2* items, int nitems, int parity,
+                                cudaStream_t s, unsigned* dev_err) {
+  if (nitems <= 0) return cudaSuccess;
+  switch (variant) {
+    case 0: return launch_t<16, 16, 4>(descs, items, nitems, parity, s, dev_err);
+    case 1: return launch_t<32, 16, 4>(descs, items, nitems, parity, s, dev_err);
+    case 2: return launch_t<32, 32, 4>(descs, items, nitems, parity, s, dev_err);
+    case 3: return launch_t<16, 32, 4>(descs, items, nitems, parity, s, dev_err);
+    case 4: return launch_t<32, 8, 4>(descs, items, nitems, parity, s, dev_err);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_repitch(const float* src, float* dst, int nx, int px,
+                           long long rows, bool to_pitched, cudaStream_t s) {
+  if (rows <= 0) return cudaSuccess;
+  const long long blocks = std::min<long long>(rows, 148LL * 16);
+  repitch_kernel<<<(unsigned)blocks, 128, 0, s>>>(src, dst, nx, px, rows,
+                                                  to_pitched);
+  return cudaGetLastError();
+}
+
+}  // namespace d3d

@@ -3,11 +3,19 @@
 // State of a request: queued -> active (its two buffers live in the device
 // arena; input copied in on the copy stream) -> retiring (its result is
 // being copied to the caller's host buffer) -> done.  A tick advances every
-// active solve by up to `chunk` steps with the multi-grid step kernel, the
-// same kernel the batch API uses: within a tick, solves are ordered by
-// steps remaining so the ones still stepping at sub-step j are a prefix of
-// the work list.  At most two ticks are in flight; their descriptor/work
-// lists use alternating staging buffers.
+// active solve by up to `chunk` steps with one multi-grid step launch per
+// sub-step: within a tick, solves are ordered by steps remaining so the
+// ones still stepping at sub-step j are a prefix of the work list, and
+// large grids are cut into z slabs so a few big solves still fill the GPU.
+// At most two ticks are in flight; their descriptor/work lists use
+// alternating staging buffers.
+//
+// Step kernel.  By default the pitched TMA kernel (d3d_pitched.cu): each
+// solve is stored with rows padded to a 16-byte pitch and read through two
+// tensor maps encoded at admission.  Host copies stay dense and contiguous
+// (one transfer each way); a device pass spreads an input into the pitched
+// layout (filling the pads) and packs a result back.  d3d_server_set_kernel(-1)
+// selects the unpadded march kernel of the batch API instead.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -22,6 +30,9 @@
 namespace {
 
 constexpr unsigned long long kAlign = 64;  // elements (256 bytes)
+constexpr int kDefaultKernel = 3;          // pitched 64 x 32 tiles
+constexpr int kMaxLanes = 4;               // compute streams
+constexpr int kDefaultLanes = 4;
 
 // First-fit allocator over the arena, in elements.
 class ArenaAlloc {
@@ -71,28 +82,36 @@ class ArenaAlloc {
 };
 
 struct Request {
+  CUtensorMap map[2];  // pitched kernel: the fields at off_a and off_b
   long long id;
   int nx, ny, nz, steps, done;
+  int px;  // row pitch in floats (nx, or nx rounded up to 4 when pitched)
+  int zc = 0, tiles = 0;  // this tick: planes per z slab, work items
+  int lane = 0;           // compute stream that runs all its steps
   float coeff[7];
   const float* host_in;
   float* host_out;
   unsigned long long off_a = 0, off_b = 0;
   bool cur_a = true;  // which buffer holds the current field
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
-  unsigned long long points() const {
-    return (unsigned long long)nx * ny * nz;
+  unsigned long long elems() const {
+    return (unsigned long long)px * ny * nz;
   }
 };
 
-// Staging for one tick's descriptors and work items (pinned + device).
+// Staging for one tick's descriptors (BatchDesc or PitchedDesc, by the
+// server's kernel) and work items, pinned + device.
 struct Staging {
-  d3d::BatchDesc* h_desc = nullptr;
+  void* h_desc = nullptr;
   int2* h_items = nullptr;
-  d3d::BatchDesc* d_desc = nullptr;
+  void* d_desc = nullptr;
   int2* d_items = nullptr;
-  size_t cap_desc = 0, cap_items = 0;
-  cudaEvent_t done = nullptr;  // recorded after the tick's kernels
+  size_t cap_desc = 0, cap_items = 0;  // bytes, items
+  // Per lane: recorded before and after the lane's step launches.
+  cudaEvent_t start[kMaxLanes] = {}, done[kMaxLanes] = {};
+  bool used[kMaxLanes] = {};
   bool in_flight = false;
+  bool timed = false;  // not yet added to the step time
 };
 
 }  // namespace
@@ -102,15 +121,21 @@ struct d3d_server_s {
   unsigned long long arena_elems = 0;
   ArenaAlloc alloc;
   int chunk = 8;
+  int kernel = kDefaultKernel;  // pitched variant, or -1: march kernel
   std::deque<Request*> queued;
   std::vector<Request*> active;
   std::vector<Request*> retiring;
-  cudaStream_t compute = nullptr, copy = nullptr;
+  // Solves are spread over `lanes` compute streams (each solve stays on
+  // one), so one lane's launch tail overlaps another lane's work.
+  cudaStream_t lane[kMaxLanes] = {};
+  int lanes = kDefaultLanes;
+  cudaStream_t copy = nullptr;
   Staging stage[2];
   int tick_index = 0;
   int device = 0;
   long long next_id = 0;
   long long submitted = 0, completed = 0, ticks = 0;
+  double step_ms = 0.0;  // device time of the step launches
   unsigned long long launches = 0, peak_used = 0;
 };
 
@@ -124,14 +149,14 @@ int sfail(int code, const char* msg) { return d3d::set_error(code, "%s", msg); }
     if (e__ != cudaSuccess) return d3d::set_cuda_error(e__, what);    \
   } while (0)
 
-int ensure_staging(Staging& st, size_t ndesc, size_t nitems) {
-  if (ndesc > st.cap_desc) {
+int ensure_staging(Staging& st, size_t desc_bytes, size_t nitems) {
+  if (desc_bytes > st.cap_desc) {
     if (st.h_desc) cudaFreeHost(st.h_desc);
     if (st.d_desc) cudaFree(st.d_desc);
-    st.cap_desc = std::max(ndesc, 2 * st.cap_desc);
-    S_TRY(cudaMallocHost(&st.h_desc, st.cap_desc * sizeof(d3d::BatchDesc)),
+    st.cap_desc = std::max(desc_bytes, 2 * st.cap_desc);
+    S_TRY(cudaMallocHost(&st.h_desc, st.cap_desc),
           "cudaMallocHost (server staging)");
-    S_TRY(cudaMalloc(&st.d_desc, st.cap_desc * sizeof(d3d::BatchDesc)),
+    S_TRY(cudaMalloc(&st.d_desc, st.cap_desc),
           "cudaMalloc (server staging)");
   }
   if (nitems > st.cap_items) {
@@ -149,21 +174,37 @@ int ensure_staging(Staging& st, size_t ndesc, size_t nitems) {
 void free_request(d3d_server s, Request* r) {
   if (r->ev_in) cudaEventDestroy(r->ev_in);
   if (r->ev_out) cudaEventDestroy(r->ev_out);
-  s->alloc.release(r->off_a, r->points());
-  s->alloc.release(r->off_b, r->points());
+  s->alloc.release(r->off_a, r->elems());
+  s->alloc.release(r->off_b, r->elems());
   delete r;
 }
 
-// Starts the device->host copy of a finished solve.
+size_t dense_bytes(const Request* r) {
+  return (size_t)r->nx * r->ny * r->nz * sizeof(float);
+}
+
+// Starts the device->host copy of a finished solve.  A pitched result is
+// first made dense in the solve's other buffer (one device pass), so the
+// copy to the host is one contiguous transfer.
 int start_retire(d3d_server s, Request* r) {
+  const float* src = s->arena + (r->cur_a ? r->off_a : r->off_b);
+  if (r->px != r->nx) {
+    float* dense = s->arena + (r->cur_a ? r->off_b : r->off_a);
+    S_TRY(d3d::launch_repitch(src, dense, r->nx, r->px,
+                              (long long)r->ny * r->nz, false,
+                              s->lane[r->lane]),
+          "dense copy of a result");
+    ++s->launches;
+    d3d::note_launches(1);
+    src = dense;
+  }
   cudaEvent_t ready;
   S_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming),
         "cudaEventCreate");
-  S_TRY(cudaEventRecord(ready, s->compute), "cudaEventRecord");
+  S_TRY(cudaEventRecord(ready, s->lane[r->lane]), "cudaEventRecord");
   S_TRY(cudaStreamWaitEvent(s->copy, ready, 0), "cudaStreamWaitEvent");
   cudaEventDestroy(ready);
-  const float* src = s->arena + (r->cur_a ? r->off_a : r->off_b);
-  S_TRY(cudaMemcpyAsync(r->host_out, src, r->points() * sizeof(float),
+  S_TRY(cudaMemcpyAsync(r->host_out, src, dense_bytes(r),
                         cudaMemcpyDeviceToHost, s->copy),
         "D2H copy (result)");
   S_TRY(cudaEventCreateWithFlags(&r->ev_out, cudaEventDisableTiming),
@@ -174,28 +215,59 @@ int start_retire(d3d_server s, Request* r) {
 }
 
 int admit(d3d_server s) {
+  // Outstanding point-steps per lane; a new solve joins the lightest.
+  double work[kMaxLanes] = {};
+  for (const Request* r : s->active)
+    work[r->lane] += (double)r->elems() * (r->steps - r->done);
   for (auto it = s->queued.begin(); it != s->queued.end();) {
     Request* r = *it;
     unsigned long long a, b;
-    if (!s->alloc.alloc(r->points(), &a)) {
+    if (!s->alloc.alloc(r->elems(), &a)) {
       ++it;
       continue;
     }
-    if (!s->alloc.alloc(r->points(), &b)) {
-      s->alloc.release(a, r->points());
+    if (!s->alloc.alloc(r->elems(), &b)) {
+      s->alloc.release(a, r->elems());
       ++it;
       continue;
     }
     r->off_a = a;
     r->off_b = b;
-    S_TRY(cudaMemcpyAsync(s->arena + a, r->host_in,
-                          r->points() * sizeof(float),
+    if (s->kernel >= 0) {
+      const int bxm = d3d::pitched_box_x(s->kernel);
+      const int bym = d3d::pitched_box_y(s->kernel);
+      for (int m = 0; m < 2; ++m) {
+        cudaError_t e = d3d::encode_field_map(
+            &r->map[m], s->arena + (m ? b : a), r->px, r->ny, r->nz,
+            d3d::kF32, bxm, bym);
+        if (e != cudaSuccess) {
+          s->alloc.release(a, r->elems());
+          s->alloc.release(b, r->elems());
+          return d3d::set_cuda_error(e, "tensor map of a served solve");
+        }
+      }
+    }
+    // The input lands dense; a pitched solve lands in its b buffer and is
+    // spread into a (pads filled) by one device pass on the copy stream.
+    float* land = s->arena + (r->px != r->nx ? b : a);
+    S_TRY(cudaMemcpyAsync(land, r->host_in, dense_bytes(r),
                           cudaMemcpyHostToDevice, s->copy),
           "H2D copy (input)");
+    if (r->px != r->nx) {
+      S_TRY(d3d::launch_repitch(land, s->arena + a, r->nx, r->px,
+                                (long long)r->ny * r->nz, true, s->copy),
+            "pitched copy of an input");
+      ++s->launches;
+      d3d::note_launches(1);
+    }
     S_TRY(cudaEventCreateWithFlags(&r->ev_in, cudaEventDisableTiming),
           "cudaEventCreate");
     S_TRY(cudaEventRecord(r->ev_in, s->copy), "cudaEventRecord");
-    S_TRY(cudaStreamWaitEvent(s->compute, r->ev_in, 0),
+    r->lane = 0;
+    for (int l = 1; l < s->lanes; ++l)
+      if (work[l] < work[r->lane]) r->lane = l;
+    work[r->lane] += (double)r->elems() * r->steps;
+    S_TRY(cudaStreamWaitEvent(s->lane[r->lane], r->ev_in, 0),
           "cudaStreamWaitEvent");
     it = s->queued.erase(it);
     if (r->steps == 0) {
@@ -209,65 +281,185 @@ int admit(d3d_server s) {
   return D3D_OK;
 }
 
+// z slabs: planes per work item are capped at kMaxSlab (long marches make
+// one launch wait for its slowest CTAs); while a tick's launch would have
+// fewer than kSlabTarget work items the cap halves, down to kMinSlab
+// planes (each slab re-reads the plane above and below it).
+constexpr long kSlabTarget = 8 * 148;
+constexpr int kMaxSlab = 32, kMinSlab = 16;
+int slab_planes(int nz, int cap) {
+  const int ns = (nz + cap - 1) / cap;
+  return (nz + ns - 1) / ns;  // balanced slabs of at most `cap` planes
+}
+
+// Adds a finished tick's step time to the counters (once): the span from
+// its first lane's start to its last lane's end.
+void harvest(d3d_server s, Staging& st) {
+  if (!st.timed) return;
+  int first = -1, last = -1;
+  for (int l = 0; l < kMaxLanes; ++l) {
+    if (!st.used[l]) continue;
+    if (cudaEventQuery(st.done[l]) != cudaSuccess) return;
+    float ms = 0.0f;
+    if (first < 0 ||
+        (cudaEventElapsedTime(&ms, st.start[l], st.start[first]) ==
+             cudaSuccess &&
+         ms > 0.0f))
+      first = l;
+    if (last < 0 ||
+        (cudaEventElapsedTime(&ms, st.done[last], st.done[l]) ==
+             cudaSuccess &&
+         ms > 0.0f))
+      last = l;
+  }
+  float ms = 0.0f;
+  if (first >= 0 &&
+      cudaEventElapsedTime(&ms, st.start[first], st.done[last]) ==
+          cudaSuccess)
+    s->step_ms += ms;
+  st.timed = false;
+}
+
+// Waits for every lane of a staging's tick.
+int wait_staging(d3d_server s, Staging& st) {
+  for (int l = 0; l < kMaxLanes; ++l)
+    if (st.used[l])
+      S_TRY(cudaEventSynchronize(st.done[l]), "cudaEventSynchronize");
+  harvest(s, st);
+  for (bool& u : st.used) u = false;
+  st.in_flight = false;
+  return D3D_OK;
+}
+
 int advance(d3d_server s) {
   if (s->active.empty()) return D3D_OK;
   Staging& st = s->stage[s->tick_index & 1];
   if (st.in_flight) {
-    S_TRY(cudaEventSynchronize(st.done), "cudaEventSynchronize");
-    st.in_flight = false;
+    int rc = wait_staging(s, st);
+    if (rc) return rc;
   }
   std::vector<Request*>& act = s->active;
-  std::sort(act.begin(), act.end(), [](const Request* x, const Request* y) {
-    return x->steps - x->done > y->steps - y->done;
-  });
-  const d3d::BShape sh = d3d::kBShapes[0];
-  size_t nitems = 0;
-  std::vector<int> tiles(act.size());
-  for (size_t i = 0; i < act.size(); ++i) {
-    const Request* r = act[i];
-    tiles[i] = ((r->nx + sh.bx - 1) / sh.bx) * ((r->ny + sh.by - 1) / sh.by);
-    nitems += tiles[i];
+  const bool pitched = s->kernel >= 0;
+  int bx = d3d::kBShapes[0].bx, by = d3d::kBShapes[0].by;
+  if (pitched) {
+    bx = 4 * d3d::pitched_variant(s->kernel).lanes;
+    by = d3d::pitched_variant(s->kernel).by;
   }
-  int rc = ensure_staging(st, act.size(), nitems);
+  size_t nitems = 0;
+  for (int cap = kMaxSlab;; cap /= 2) {
+    nitems = 0;
+    for (Request* r : act) {
+      const int txy = ((r->nx + bx - 1) / bx) * ((r->ny + by - 1) / by);
+      r->zc = slab_planes(r->nz, cap);
+      r->tiles = txy * ((r->nz + r->zc - 1) / r->zc);
+      nitems += r->tiles;
+    }
+    if ((long)nitems >= kSlabTarget || cap / 2 < kMinSlab) break;
+  }
+  // Each lane's solves are contiguous.  Within a lane, the solves still
+  // stepping at sub-step j must be a prefix: order by the steps this tick
+  // runs, then by slab depth, longest first, so a launch starts its
+  // longest CTAs first and its tail is short.
+  const int chunk = s->chunk;
+  std::sort(act.begin(), act.end(), [chunk](const Request* x,
+                                            const Request* y) {
+    if (x->lane != y->lane) return x->lane < y->lane;
+    const int nx_ = std::min(chunk, x->steps - x->done);
+    const int ny_ = std::min(chunk, y->steps - y->done);
+    if (nx_ != ny_) return nx_ > ny_;
+    return x->zc > y->zc;
+  });
+  const size_t desc_size =
+      pitched ? sizeof(d3d::PitchedDesc) : sizeof(d3d::BatchDesc);
+  int rc = ensure_staging(st, act.size() * desc_size, nitems);
   if (rc) return rc;
-  std::vector<int> active_at(s->chunk, 0);
+  // Per lane: first descriptor, first item, items active at sub-step j.
+  size_t desc0[kMaxLanes + 1] = {}, item0[kMaxLanes + 1] = {};
+  std::vector<int> active_at((size_t)kMaxLanes * s->chunk, 0);
   size_t k = 0;
   for (size_t i = 0; i < act.size(); ++i) {
     Request* r = act[i];
-    d3d::BatchDesc& d = st.h_desc[i];
-    d.a = s->arena + (r->cur_a ? r->off_a : r->off_b);
-    d.b = s->arena + (r->cur_a ? r->off_b : r->off_a);
-    d.nx = r->nx;
-    d.ny = r->ny;
-    d.nz = r->nz;
-    d.tiles_x = (r->nx + sh.bx - 1) / sh.bx;
-    for (int j = 0; j < 7; ++j) d.k[j] = r->coeff[j];
-    d.k[7] = -0.0f;
-    for (int t = 0; t < tiles[i]; ++t) st.h_items[k++] = make_int2((int)i, t);
+    for (int l = r->lane + 1; l <= kMaxLanes; ++l) {
+      desc0[l] = i + 1;
+      item0[l] = k + r->tiles;
+    }
+    float* cur = s->arena + (r->cur_a ? r->off_a : r->off_b);
+    float* nxt = s->arena + (r->cur_a ? r->off_b : r->off_a);
+    const int tiles_x = (r->nx + bx - 1) / bx;
+    const int tiles_xy = tiles_x * ((r->ny + by - 1) / by);
+    if (pitched) {
+      d3d::PitchedDesc& d = static_cast<d3d::PitchedDesc*>(st.h_desc)[i];
+      d.map[0] = r->map[r->cur_a ? 0 : 1];
+      d.map[1] = r->map[r->cur_a ? 1 : 0];
+      d.a = cur;
+      d.b = nxt;
+      d.nx = r->nx;
+      d.px = r->px;
+      d.ny = r->ny;
+      d.nz = r->nz;
+      d.tiles_x = tiles_x;
+      d.tiles_xy = tiles_xy;
+      d.zc = r->zc;
+      d.unused = 0;
+      for (int j = 0; j < 7; ++j) d.k[j] = r->coeff[j];
+      d.k[7] = -0.0f;
+    } else {
+      d3d::BatchDesc& d = static_cast<d3d::BatchDesc*>(st.h_desc)[i];
+      d.a = cur;
+      d.b = nxt;
+      d.nx = r->nx;
+      d.ny = r->ny;
+      d.nz = r->nz;
+      d.tiles_x = tiles_x;
+      d.tiles_xy = tiles_xy;
+      d.zc = r->zc;
+      for (int j = 0; j < 7; ++j) d.k[j] = r->coeff[j];
+      d.k[7] = -0.0f;
+    }
+    for (int t = 0; t < r->tiles; ++t) st.h_items[k++] = make_int2((int)i, t);
     const int n = std::min(s->chunk, r->steps - r->done);
-    for (int j = 0; j < n; ++j) active_at[j] += tiles[i];
+    for (int j = 0; j < n; ++j)
+      active_at[(size_t)r->lane * s->chunk + j] += r->tiles;
   }
-  S_TRY(cudaMemcpyAsync(st.d_desc, st.h_desc,
-                        act.size() * sizeof(d3d::BatchDesc),
-                        cudaMemcpyHostToDevice, s->compute),
-        "H2D descriptors");
-  S_TRY(cudaMemcpyAsync(st.d_items, st.h_items, nitems * sizeof(int2),
-                        cudaMemcpyHostToDevice, s->compute),
-        "H2D work items");
+  // Each lane copies its own descriptors and items and launches its
+  // sub-steps on its stream; lanes never wait for one another.
   unsigned long long n_launch = 0;
-  for (int j = 0; j < s->chunk && active_at[j] > 0; ++j) {
-    S_TRY(d3d::launch_batch_step(0, st.d_desc, st.d_items, active_at[j],
-                                 j & 1, s->compute),
-          "server step launch");
-    ++n_launch;
+  for (int l = 0; l < s->lanes; ++l) {
+    const size_t nd = desc0[l + 1] - desc0[l], ni = item0[l + 1] - item0[l];
+    if (nd == 0) continue;
+    cudaStream_t ls = s->lane[l];
+    char* hd = static_cast<char*>(st.h_desc) + desc0[l] * desc_size;
+    char* dd = static_cast<char*>(st.d_desc) + desc0[l] * desc_size;
+    S_TRY(cudaMemcpyAsync(dd, hd, nd * desc_size, cudaMemcpyHostToDevice, ls),
+          "H2D descriptors");
+    S_TRY(cudaMemcpyAsync(st.d_items + item0[l], st.h_items + item0[l],
+                          ni * sizeof(int2), cudaMemcpyHostToDevice, ls),
+          "H2D work items");
+    if (!st.start[l]) {
+      S_TRY(cudaEventCreate(&st.start[l]), "cudaEventCreate");
+      S_TRY(cudaEventCreate(&st.done[l]), "cudaEventCreate");
+    }
+    S_TRY(cudaEventRecord(st.start[l], ls), "cudaEventRecord");
+    const int* act_l = active_at.data() + (size_t)l * s->chunk;
+    for (int j = 0; j < s->chunk && act_l[j] > 0; ++j) {
+      S_TRY(pitched
+                ? d3d::launch_pitched_step(
+                      s->kernel, static_cast<d3d::PitchedDesc*>(st.d_desc),
+                      st.d_items + item0[l], act_l[j], j & 1, ls,
+                      d3d::device_error_word())
+                : d3d::launch_batch_step(
+                      0, static_cast<d3d::BatchDesc*>(st.d_desc),
+                      st.d_items + item0[l], act_l[j], j & 1, ls),
+            "server step launch");
+      ++n_launch;
+    }
+    S_TRY(cudaEventRecord(st.done[l], ls), "cudaEventRecord");
+    st.used[l] = true;
   }
   s->launches += n_launch;
   d3d::note_launches(n_launch);
-  if (!st.done)
-    S_TRY(cudaEventCreateWithFlags(&st.done, cudaEventDisableTiming),
-          "cudaEventCreate");
-  S_TRY(cudaEventRecord(st.done, s->compute), "cudaEventRecord");
   st.in_flight = true;
+  st.timed = true;
   ++s->tick_index;
   // Book-keeping, then start the copies of the solves that finished.
   std::vector<Request*> still;
@@ -300,8 +492,8 @@ int d3d_server_create(size_t arena_bytes, int chunk, d3d_server* out) {
   s->chunk = chunk;
   s->arena_elems = arena_bytes / sizeof(float) / kAlign * kAlign;
   cudaError_t e = cudaMalloc(&s->arena, s->arena_elems * sizeof(float));
-  if (e == cudaSuccess)
-    e = cudaStreamCreateWithFlags(&s->compute, cudaStreamNonBlocking);
+  for (int l = 0; l < kMaxLanes && e == cudaSuccess; ++l)
+    e = cudaStreamCreateWithFlags(&s->lane[l], cudaStreamNonBlocking);
   if (e == cudaSuccess)
     e = cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
@@ -321,13 +513,15 @@ int d3d_server_submit(d3d_server s, int nx, int ny, int nz, int steps,
   if (nx < 1 || ny < 1 || nz < 1 || steps < 0 ||
       (long long)nx * ny >= (1LL << 31))
     return sfail(D3D_E_INVALID, "bad grid dimensions or steps");
-  const unsigned long long pts = (unsigned long long)nx * ny * nz;
+  const int px = s->kernel >= 0 ? (nx + 3) / 4 * 4 : nx;
+  const unsigned long long pts = (unsigned long long)px * ny * nz;
   const unsigned long long need = 2 * ((pts + kAlign - 1) / kAlign * kAlign);
   if (need > s->arena_elems)
     return sfail(D3D_E_BUSY, "solve larger than the server's arena");
   Request* r = new (std::nothrow) Request();
   if (!r) return sfail(D3D_E_OOM, "request allocation");
   r->id = s->next_id++;
+  r->px = px;
   r->nx = nx;
   r->ny = ny;
   r->nz = nz;
@@ -374,6 +568,26 @@ int d3d_server_tick(d3d_server s, long long* done_ids, int max_done,
   return D3D_OK;
 }
 
+int d3d_server_set_kernel(d3d_server s, int kernel) {
+  if (!s) return sfail(D3D_E_INVALID, "NULL server");
+  if (kernel < -1 || kernel >= d3d::kNumPitchedVariants)
+    return sfail(D3D_E_INVALID, "no such server kernel");
+  if (!s->queued.empty() || !s->active.empty() || !s->retiring.empty())
+    return sfail(D3D_E_BUSY, "the step kernel changes only on an idle server");
+  s->kernel = kernel;
+  return D3D_OK;
+}
+
+int d3d_server_set_lanes(d3d_server s, int lanes) {
+  if (!s) return sfail(D3D_E_INVALID, "NULL server");
+  if (lanes < 1 || lanes > kMaxLanes)
+    return sfail(D3D_E_INVALID, "lanes must be 1 to 4");
+  if (!s->queued.empty() || !s->active.empty() || !s->retiring.empty())
+    return sfail(D3D_E_BUSY, "lanes change only on an idle server");
+  s->lanes = lanes;
+  return D3D_OK;
+}
+
 int d3d_server_pending(d3d_server s, int* queued, int* active,
                        int* retiring) {
   if (!s) return sfail(D3D_E_INVALID, "NULL server");
@@ -385,18 +599,22 @@ int d3d_server_pending(d3d_server s, int* queued, int* active,
 
 int d3d_server_stats(d3d_server s, char* buf, size_t len) {
   if (!s || !buf) return sfail(D3D_E_INVALID, "NULL argument");
+  for (auto& st : s->stage) harvest(s, st);
   snprintf(buf, len,
            "{\"submitted\": %lld, \"completed\": %lld, \"ticks\": %lld, "
-           "\"launches\": %llu, \"chunk\": %d, \"arena_bytes\": %llu, "
-           "\"peak_arena_bytes\": %llu}",
+           "\"launches\": %llu, \"chunk\": %d, \"kernel\": %d, "
+           "\"lanes\": %d, "
+           "\"step_ms\": %.4f, "
+           "\"arena_bytes\": %llu, \"peak_arena_bytes\": %llu}",
            s->submitted, s->completed, s->ticks, s->launches, s->chunk,
-           s->arena_elems * 4ULL, s->peak_used * 4ULL);
+           s->kernel, s->lanes, s->step_ms, s->arena_elems * 4ULL, s->peak_used * 4ULL);
   return D3D_OK;
 }
 
 int d3d_server_destroy(d3d_server s) {
   if (!s) return D3D_OK;
-  if (s->compute) cudaStreamSynchronize(s->compute);
+  for (cudaStream_t l : s->lane)
+    if (l) cudaStreamSynchronize(l);
   if (s->copy) cudaStreamSynchronize(s->copy);
   for (Request* r : s->queued) delete r;
   for (Request* r : s->active) free_request(s, r);
@@ -406,10 +624,14 @@ int d3d_server_destroy(d3d_server s) {
     if (st.h_items) cudaFreeHost(st.h_items);
     if (st.d_desc) cudaFree(st.d_desc);
     if (st.d_items) cudaFree(st.d_items);
-    if (st.done) cudaEventDestroy(st.done);
+    for (int l = 0; l < kMaxLanes; ++l) {
+      if (st.start[l]) cudaEventDestroy(st.start[l]);
+      if (st.done[l]) cudaEventDestroy(st.done[l]);
+    }
   }
   if (s->arena) cudaFree(s->arena);
-  if (s->compute) cudaStreamDestroy(s->compute);
+  for (cudaStream_t l : s->lane)
+    if (l) cudaStreamDestroy(l);
   if (s->copy) cudaStreamDestroy(s->copy);
   delete s;
   return D3D_OK;

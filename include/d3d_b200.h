@@ -274,7 +274,8 @@ int d3d_batch_destroy(d3d_batch batch);
  *      server's device arena (its HBM budget), copying their inputs in on a
  *      copy stream,
  *   3. advances every active solve by up to `chunk` steps with the
- *      multi-grid step kernel (solves admitted this tick included), and
+ *      multi-grid step kernel (solves admitted this tick included; by
+ *      default a TMA kernel over row-padded copies of the fields), and
  *   4. starts the device->host copy of every solve that just finished.
  * Requests that arrive while others run join at the next tick; their work
  * overlaps on the device.  Each solve's arithmetic is RunKernel's, so its
@@ -288,7 +289,8 @@ typedef struct d3d_server_s* d3d_server;
 int d3d_server_create(size_t arena_bytes, int chunk, d3d_server* out);
 
 /* Queues one solve; *id receives its request id.  D3D_E_BUSY if the solve
- * can never fit the arena (2 * nx*ny*nz floats > arena). */
+ * can never fit the arena (2 * ceil4(nx)*ny*nz floats > arena with the
+ * default kernel; 2 * nx*ny*nz with the march kernel). */
 int d3d_server_submit(d3d_server server, int nx, int ny, int nz, int steps,
                       const float coeff[7], const float* host_in,
                       float* host_out, long long* id);
@@ -298,11 +300,27 @@ int d3d_server_submit(d3d_server server, int nx, int ny, int nz, int steps,
 int d3d_server_tick(d3d_server server, long long* done_ids, int max_done,
                     int* n_done);
 
+/* The step kernel of an idle server (D3D_E_BUSY otherwise): 0..4 the
+ * pitched TMA kernel's tile shapes (0: 64 x 16, 1: 128 x 16, 2: 128 x 32,
+ * 3: 64 x 32 (default), 4: 128 x 8), -1 the batch API's march kernel.
+ * With the TMA kernel each solve is stored with rows padded to a multiple
+ * of 4 floats, so it takes 2 * ceil4(nx)*ny*nz floats of the arena. */
+int d3d_server_set_kernel(d3d_server server, int kernel);
+
+/* Compute streams of an idle server (1..4, default 4; D3D_E_BUSY when
+ * not idle).  Each solve runs all its steps on one stream, picked at
+ * admission as the one with the least outstanding work; streams never wait
+ * for one another, so one stream's launch tail overlaps another's work. */
+int d3d_server_set_lanes(d3d_server server, int lanes);
+
 /* Number of requests queued, active on the device and copying out. */
 int d3d_server_pending(d3d_server server, int* queued, int* active,
                        int* retiring);
 
-/* JSON counters: submitted, completed, ticks, launches, peak arena use. */
+/* JSON counters: submitted, completed, ticks, launches, chunk, kernel,
+ * lanes, step_ms (device time of the step launches from CUDA events: per
+ * tick, first stream's start to last stream's end), arena size and peak
+ * arena use. */
 int d3d_server_stats(d3d_server server, char* buf, size_t len);
 
 int d3d_server_destroy(d3d_server server);

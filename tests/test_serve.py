@@ -25,8 +25,9 @@ def _requests(seed, n, max_side=48, max_steps=40, cubic=False):
     return reqs
 
 
-def _serve(reqs, arena_bytes=1 << 28, chunk=8, interleave=False):
-    server = B.Server(arena_bytes, chunk)
+def _serve(reqs, arena_bytes=1 << 28, chunk=8, interleave=False,
+           kernel=None, lanes=None):
+    server = B.Server(arena_bytes, chunk, kernel, lanes)
     outs = [np.full_like(f, np.nan) for f, _, _ in reqs]
     ids = {}
     done = set()
@@ -55,6 +56,68 @@ def test_same_alone_and_in_the_mix():
     for k in (0, 4, 9, 17):
         alone, _ = _serve([reqs[k]])
         assert alone[0].tobytes() == mixed[k].tobytes()
+
+
+@pytest.mark.parametrize("kernel,lanes", [(-1, 1), (-1, 2), (0, 3), (1, 1),
+                                          (1, 2), (2, 4), (3, 2), (4, 1)])
+def test_every_step_kernel_bit_exact(kernel, lanes):
+    """Each tile shape of the pitched TMA kernel and the march kernel, on
+    1 to 4 compute streams, on grids whose nx leaves 0..3 pad columns
+    (nx = 1 included), single rows and planes, and grids deeper than one z
+    slab."""
+    dims = [(1, 1, 1), (1, 7, 5), (2, 3, 40), (3, 1, 9), (5, 33, 17),
+            (8, 8, 8), (13, 17, 19), (64, 16, 3), (130, 9, 35),
+            (131, 70, 6), (257, 5, 4), (36, 35, 70)]
+    reqs = []
+    for i, (nx, ny, nz) in enumerate(dims):
+        c = B.batch_coefficients(nx, ny, nz, 0.05 + 0.01 * i)
+        f = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), 70 + i)
+        reqs.append((f, (i * 7) % 13, c))
+    outs, stats = _serve(reqs, chunk=5, interleave=True, kernel=kernel,
+                         lanes=lanes)
+    assert stats["kernel"] == kernel and stats["lanes"] == lanes
+    for (f, steps, c), o in zip(reqs, outs):
+        assert o.tobytes() == O.run(f, c, steps).tobytes()
+    assert B.check_device_errors() == 0
+
+
+def test_kernel_and_lanes_change_only_when_idle():
+    server = B.Server(1 << 24, 4)
+    f = np.zeros((4, 4, 5), np.float32)
+    o = np.empty_like(f)
+    server.submit(f, o, 3, B.batch_coefficients(5, 4, 4, 0.1))
+    with pytest.raises(B.D3DError) as ei:
+        server.set_kernel(-1)
+    assert ei.value.code == B.D3D_E_BUSY
+    with pytest.raises(B.D3DError) as ei:
+        server.set_lanes(1)
+    assert ei.value.code == B.D3D_E_BUSY
+    server.drain()
+    server.set_kernel(-1)
+    server.set_lanes(3)
+    for bad in (0, 5):
+        with pytest.raises(B.D3DError):
+            server.set_lanes(bad)
+    with pytest.raises(B.D3DError):
+        server.set_kernel(5)
+    server.close()
+
+
+def test_large_grids_cut_into_z_slabs():
+    """Grids deep enough to be cut into z slabs (one alone, then beside
+    small ones); odd depths leave a short last slab."""
+    dims = [(150, 70, 101), (33, 9, 200), (64, 64, 47), (7, 5, 31)]
+    reqs = []
+    for i, (nx, ny, nz) in enumerate(dims):
+        c = B.batch_coefficients(nx, ny, nz, 0.1 + 0.02 * i)
+        f = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), 40 + i)
+        reqs.append((f, 5 + 2 * i, c))
+    alone, _ = _serve(reqs[:1], chunk=3)
+    f0, st0, c0 = reqs[0]
+    assert alone[0].tobytes() == O.run(f0, c0, st0).tobytes()
+    outs, _ = _serve(reqs, chunk=4, interleave=True)
+    for (f, steps, c), o in zip(reqs, outs):
+        assert o.tobytes() == O.run(f, c, steps).tobytes()
 
 
 @pytest.mark.parametrize("chunk", [1, 3, 16])
