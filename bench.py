@@ -613,12 +613,32 @@ def main():
                     help="skip the CPU baseline leg")
     ap.add_argument("--no-side", action="store_true",
                     help="skip the batched, serving and 2D legs")
+    ap.add_argument("--only-leg", choices=["batched", "serving",
+                                           "diffusion2d"],
+                    help="run one side leg alone on GPU 0 and print its "
+                         "JSON (no headline line; for profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.only_leg:
+        return run_one_leg(args.only_leg)
     return run_b200(args)
+
+
+def run_one_leg(leg):
+    import torch
+    import benchmarks_b200 as B
+    torch.cuda.set_device(0)
+    if leg == "batched":
+        out = batched_leg(B, torch)
+    elif leg == "serving":
+        out = serving_leg(B, torch)
+    else:
+        out = diffusion2d_leg(B, torch, torch.cuda.current_stream())
+    print(json.dumps({"leg": leg, **out}), flush=True)
+    return 0
 
 
 if __name__ == "__main__":
