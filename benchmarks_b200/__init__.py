@@ -510,7 +510,8 @@ class Server:
 
     def set_kernel(self, kernel):
         """Step kernel of the idle server: 0..4 the pitched TMA kernel's
-        tile shapes (3 is the default), -1 the batch API's march kernel."""
+        tile shapes, 5 and 6 its strip form with 1 or 2 segments a thread
+        (6 is the default), -1 the batch API's march kernel."""
         check(lib().d3d_server_set_kernel(self._h, int(kernel)))
 
     def set_lanes(self, lanes):

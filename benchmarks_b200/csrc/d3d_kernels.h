@@ -137,7 +137,8 @@ struct alignas(64) PitchedDesc {
   float* a;
   float* b;
   int nx, px, ny, nz, tiles_x, tiles_xy, zc, unused;
-  float k[8];  // ce, cw, cn, cs, ct, cb, cc, and -0.0
+  int seg_w, rows;  // strip form: segments per piece, rows per strip
+  float k[8];       // ce, cw, cn, cs, ct, cb, cc, and -0.0
 };
 
 // Tile shapes of the pitched kernel: `lanes` per tile row (tile width
@@ -154,6 +155,23 @@ int pitched_box_y(int v);
 cudaError_t launch_pitched_step(int variant, const PitchedDesc* descs,
                                 const int2* items, int nitems, int parity,
                                 cudaStream_t s, unsigned* dev_err);
+
+// Strip form of the pitched kernel (NR = 1 or 2 segments a thread): a CTA
+// covers `rows` whole rows of one of `pieces` near-equal pieces of the
+// pitch (segs 16-byte segments each) and a z slab; items as for the tile
+// form, with tiles_x = pieces and tiles_xy = pieces * ceil(ny / rows).
+// Tensor-map box: (4 * segs + 8) x (rows + 2).
+constexpr int kStripMaxW = 248;  // columns per piece: box width <= 256
+__host__ __device__ constexpr int strip_stage_bytes(int nr) {
+  return nr * 6656;
+}
+struct StripShape {
+  int pieces, segs, rows;
+};
+StripShape strip_shape(int px, int ny, int nr);
+cudaError_t launch_pitched_strip(int nr, const PitchedDesc* descs,
+                                 const int2* items, int nitems, int parity,
+                                 cudaStream_t s, unsigned* dev_err);
 
 // Dense rows (nx floats) -> pitched rows (px floats, pads filled from
 // column nx-1) when to_pitched, else pitched -> dense; rows = ny * nz.

@@ -19,7 +19,9 @@
 // within the row's lanes, y neighbours from shared memory, and every output
 // segment is one 16-byte store.  A row of the tile is LPR lanes wide
 // (LPR = 32: 128-column tiles; LPR = 16: 64-column tiles, two rows per warp
-// instruction), which bounds the columns wasted on narrow grids.
+// instruction), which bounds the columns wasted on narrow grids.  The strip
+// form (pitched_strip_kernel, below; the server's default) maps threads
+// onto whole rows instead, so almost no lane falls outside its grid.
 //
 // The two tensor maps of each grid (its a and b buffers) sit in the work
 // descriptors in global memory, rewritten by the host between launches; the
@@ -235,6 +237,196 @@ drain:
   __syncthreads();
 }
 
+// ---------------------------------------------------------------------------
+// Strip form.  A CTA covers `rows` whole rows of one piece of the grid's
+// width (the whole pitch when it is at most kStripMaxW columns, else
+// near-equal pieces) and a z slab.  Thread i takes the strip's (row,
+// segment) pairs with linear index r * 256 + i (r < NR), so nearly every
+// lane owns a real segment whatever the width: the tile forms above leave
+// a quarter of their lanes outside grids 32..256 wide.  x neighbours are
+// shuffles between lanes of one row; a segment at a row or warp edge reads
+// its neighbour word from the staged plane instead.  The box, and so the
+// stage, is (4 * segs + 8) x (rows + 2) floats, set per grid.
+// ---------------------------------------------------------------------------
+template <int NR, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+    pitched_strip_kernel(const PitchedDesc* __restrict__ descs,
+                         const int2* __restrict__ items, int parity,
+                         unsigned* __restrict__ dev_err) {
+  constexpr int S = 4, V = 4, HX = 4;
+  constexpr int STAGE = strip_stage_bytes(NR);
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  float* stages = reinterpret_cast<float*>(base);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + S * STAGE);
+
+  const int2 it = items[blockIdx.x];
+  const PitchedDesc* dp = descs + it.x;
+  const CUtensorMap* src = &dp->map[parity];
+  float* __restrict__ dst = parity ? dp->a : dp->b;
+  const int nx = dp->nx, px = dp->px, ny = dp->ny, nz = dp->nz;
+  const int segs = dp->seg_w, rows = dp->rows;
+  const int pw = V * segs + 2 * HX;  // shared row pitch = box width
+  const unsigned box_bytes = (unsigned)(pw * (rows + 2)) * 4u;
+  const int txy = it.y % dp->tiles_xy, zs = it.y / dp->tiles_xy;
+  const int x0 = (txy % dp->tiles_x) * V * segs;
+  const int y0 = (txy / dp->tiles_x) * rows;
+  const int z0 = zs * dp->zc;
+  const int z1 = min(nz, z0 + dp->zc);
+  if (z0 >= z1) return;
+  const Coef<float> k{dp->k[0], dp->k[1], dp->k[2], dp->k[3],
+                      dp->k[4], dp->k[5], dp->k[6], dp->k[7]};
+  const int pbase = z0 > 0 ? z0 - 1 : 0;
+  const int plast = min(z1, nz - 1);
+
+  auto stage_of = [&](int p) { return (int)((unsigned)(p - pbase) % S); };
+  auto parity_of = [&](int p) { return ((unsigned)(p - pbase) / S) & 1u; };
+  auto stage_ptr = [&](int p) {
+    return stages + stage_of(p) * (STAGE / 4);
+  };
+  auto issue = [&](int p) {
+    const int s = stage_of(p);
+    mbar_arrive_expect_tx(&bars[s], box_bytes);
+    tma_load_3d(stages + s * (STAGE / 4), src, &bars[s], x0 - HX, y0 - 1,
+                p);
+  };
+
+  if (threadIdx.x == 0) {
+    tensormap_acquire(src);
+    tma_prefetch_desc(src);
+    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int p = pbase; p <= plast && p < pbase + S; ++p) issue(p);
+  }
+
+  // Addressing.  Lanes past the strip's rows x segs pairs keep in-box
+  // offsets (their row is clamped) and store nothing.  w: x = 0 takes the
+  // centre value; a row's first segment and lane 0 read the word before
+  // the segment.  e: x = nx-1 in a full last segment takes the centre
+  // value, a padded one reads its pad (a copy of nx-1); a row's last
+  // segment and lane 31 read the word after the segment.
+  const int lane = threadIdx.x & 31;
+  int c_off[NR], n_off[NR], s_off[NR], jh[NR];
+  size_t g_off[NR];
+  bool store_ok[NR], w_sm[NR], w_own[NR], e_sm[NR], e_own[NR], cross[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    const int L = r * 256 + (int)threadIdx.x;
+    int row = L / segs;
+    const int seg = L - row * segs;
+    const bool valid = row < rows;
+    row = min(row, rows - 1);
+    const int yg = y0 + row, xg = x0 + V * seg;
+    c_off[r] = (row + 1) * pw + HX + V * seg;
+    n_off[r] = (yg == 0) ? c_off[r] : c_off[r] - pw;
+    s_off[r] = (yg >= ny - 1) ? c_off[r] : c_off[r] + pw;
+    g_off[r] = (size_t)yg * px + xg;
+    store_ok[r] = valid && yg < ny && xg < px;
+    w_own[r] = (xg == 0);
+    w_sm[r] = !w_own[r] && (seg == 0 || lane == 0);
+    e_own[r] = (xg + V - 1 == nx - 1);
+    e_sm[r] = !e_own[r] && (seg == segs - 1 || lane == 31);
+    cross[r] = (xg < nx) && (xg + V > nx);
+    jh[r] = nx - 1 - xg;
+  }
+  const size_t plane = (size_t)px * ny;
+  const Coef2 kk = coef2(k);
+
+  V16<float> q0[NR], q1[NR], q2[NR];
+  int drain_lo = pbase, drain_hi = min(plast, pbase + S - 1);
+
+  bool ok = mbar_wait_bounded(&bars[stage_of(z0)], parity_of(z0));
+  if (z0 > 0) ok = ok && mbar_wait_bounded(&bars[stage_of(z0 - 1)],
+                                           parity_of(z0 - 1));
+  if (z0 + 1 <= plast)
+    ok = ok && mbar_wait_bounded(&bars[stage_of(z0 + 1)], parity_of(z0 + 1));
+  if (!__syncthreads_and(ok)) {
+    if (threadIdx.x == 0) atomicOr(dev_err, kDevWaitTimeout);
+    goto drain;
+  }
+  {
+    const float* sc = stage_ptr(z0);
+    const float* sb = stage_ptr(pbase);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      q1[r] = ld16_shared(sc + c_off[r]);
+      q0[r] = ld16_shared(sb + c_off[r]);
+    }
+  }
+  __syncthreads();
+  if (z0 > 0 && threadIdx.x == 0 && pbase + S <= plast) issue(pbase + S);
+
+  {
+    auto step = [&](int z, const V16<float>* vb, const V16<float>* vc,
+                    V16<float>* vt) -> bool {
+      const float* sc = stage_ptr(z);
+      const float* st = stage_ptr(min(z + 1, nz - 1));
+      float* out = dst + (size_t)z * plane;
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        vt[r] = ld16_shared(st + c_off[r]);
+        const V16<float> n = ld16_shared(sc + n_off[r]);
+        const V16<float> s = ld16_shared(sc + s_off[r]);
+        float wl = __shfl_up_sync(0xffffffffu, vc[r].e[V - 1], 1);
+        float er = __shfl_down_sync(0xffffffffu, vc[r].e[0], 1);
+        wl = ld_shared_if(w_sm[r], sc + c_off[r] - 1, wl);
+        if (w_own[r]) wl = vc[r].e[0];
+        er = ld_shared_if(e_sm[r], sc + c_off[r] + V, er);
+        if (e_own[r]) er = vc[r].e[V - 1];
+        V16<float> o = point_seg<float>(kk, vc[r], n, s, vb[r], vt[r], wl, er);
+        if (cross[r]) {
+          if (jh[r] < 1) o.e[1] = o.e[0];
+          if (jh[r] < 2) o.e[2] = o.e[1];
+          o.e[3] = o.e[2];
+        }
+        if (store_ok[r]) st16_global(out + g_off[r], o);
+      }
+      bool ok2 = true;
+      if (z + 2 <= plast && z + 1 < z1)
+        ok2 = mbar_wait_bounded(&bars[stage_of(z + 2)], parity_of(z + 2));
+      if (!__syncthreads_and(ok2)) {
+        if (threadIdx.x == 0) atomicOr(dev_err, kDevWaitTimeout);
+        return false;
+      }
+      if (threadIdx.x == 0 && z + S <= plast) issue(z + S);
+      return true;
+    };
+
+    int zf = -1;
+    for (int z = z0; z < z1; z += 3) {
+      if (!step(z, q0, q1, q2)) { zf = z; break; }
+      if (z + 1 >= z1) break;
+      if (!step(z + 1, q1, q2, q0)) { zf = z + 1; break; }
+      if (z + 2 >= z1) break;
+      if (!step(z + 2, q2, q0, q1)) { zf = z + 2; break; }
+    }
+    if (zf >= 0) {
+      drain_lo = zf + 2;
+      drain_hi = min(plast, zf + S - 1);
+      goto drain;
+    }
+  }
+  return;
+
+drain:
+  if (threadIdx.x == 0) {
+    for (int p = drain_lo; p <= drain_hi; ++p) {
+      bool done = false;
+      for (unsigned i = 0; i < (kMaxWaitIters >> 4) && !done; ++i)
+        done = mbar_try_wait(&bars[stage_of(p)], parity_of(p));
+      if (!done) {
+        atomicOr(dev_err, kDevDrainTimeout);
+        break;
+      }
+    }
+  }
+  __syncthreads();
+}
+
 // Between the host's dense rows (nx floats) and the arena's pitched rows
 // (px floats): `to_pitched` writes every x in [0, px) of dst from
 // src[min(x, nx-1)], which also fills the pads; otherwise dst takes the
@@ -297,6 +489,44 @@ cudaError_t launch_pitched_step(int variant, const PitchedDesc* descs,
     case 4: return launch_t<32, 8, 4>(descs, items, nitems, parity, s, dev_err);
     default: return cudaErrorInvalidValue;
   }
+}
+
+StripShape strip_shape(int px, int ny, int nr) {
+  StripShape sh;
+  sh.pieces = (px + kStripMaxW - 1) / kStripMaxW;
+  const int w = ((px + sh.pieces - 1) / sh.pieces + 3) / 4 * 4;
+  sh.segs = w / 4;
+  sh.rows = std::max(1, std::min({64, ny, nr * 256 / sh.segs}));
+  while (sh.rows > 1 && (w + 8) * (sh.rows + 2) * 4 > strip_stage_bytes(nr))
+    --sh.rows;
+  return sh;
+}
+
+cudaError_t launch_pitched_strip(int nr, const PitchedDesc* descs,
+                                 const int2* items, int nitems, int parity,
+                                 cudaStream_t s, unsigned* dev_err) {
+  if (nitems <= 0) return cudaSuccess;
+  auto go = [&](auto kern, int smem) {
+    static bool attr_set[2] = {false, false};
+    bool& set = attr_set[nr - 1];
+    if (!set) {
+      cudaError_t e = cudaFuncSetAttribute(
+          kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e != cudaSuccess) return e;
+      set = true;
+    }
+    kern<<<nitems, 256, smem, s>>>(descs, items, parity, dev_err);
+    return cudaGetLastError();
+  };
+  // Register budgets: 64 a thread for one segment (4 CTAs/SM), 80 for two
+  // (3 CTAs/SM; at 64 it spills and measured 6% slower on B200).
+  if (nr == 1)
+    return go(pitched_strip_kernel<1, 4>,
+              4 * strip_stage_bytes(1) + 4 * 8 + 128);
+  if (nr == 2)
+    return go(pitched_strip_kernel<2, 3>,
+              4 * strip_stage_bytes(2) + 4 * 8 + 128);
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_repitch(const float* src, float* dst, int nx, int px,

@@ -10,9 +10,10 @@
 // At most two ticks are in flight; their descriptor/work lists use
 // alternating staging buffers.
 //
-// Step kernel.  By default the pitched TMA kernel (d3d_pitched.cu): each
-// solve is stored with rows padded to a 16-byte pitch and read through two
-// tensor maps encoded at admission.  Host copies stay dense and contiguous
+// Step kernel.  By default the strip form of the pitched TMA kernel
+// (d3d_pitched.cu): each solve is stored with rows padded to a 16-byte
+// pitch and read through two tensor maps encoded at admission, whose box
+// is the solve's strip (whole rows of up to 248 columns).  Host copies stay dense and contiguous
 // (one transfer each way); a device pass spreads an input into the pitched
 // layout (filling the pads) and packs a result back.  d3d_server_set_kernel(-1)
 // selects the unpadded march kernel of the batch API instead.
@@ -30,7 +31,11 @@
 namespace {
 
 constexpr unsigned long long kAlign = 64;  // elements (256 bytes)
-constexpr int kDefaultKernel = 3;          // pitched 64 x 32 tiles
+// Kernels 5 and 6: the strip form with 1 or 2 segments a thread.
+constexpr int kStripBase = d3d::kNumPitchedVariants;
+constexpr int kDefaultKernel = kStripBase + 1;  // strip, 2 segments
+constexpr int kMaxKernel = kStripBase + 1;
+int strip_nr(int kernel) { return kernel >= kStripBase ? kernel - kStripBase + 1 : 0; }
 constexpr int kMaxLanes = 4;               // compute streams
 constexpr int kDefaultLanes = 4;
 
@@ -86,6 +91,7 @@ struct Request {
   long long id;
   int nx, ny, nz, steps, done;
   int px;  // row pitch in floats (nx, or nx rounded up to 4 when pitched)
+  d3d::StripShape strip{};  // strip kernels: pieces, segments, rows
   int zc = 0, tiles = 0;  // this tick: planes per z slab, work items
   int lane = 0;           // compute stream that runs all its steps
   float coeff[7];
@@ -121,7 +127,7 @@ struct d3d_server_s {
   unsigned long long arena_elems = 0;
   ArenaAlloc alloc;
   int chunk = 8;
-  int kernel = kDefaultKernel;  // pitched variant, or -1: march kernel
+  int kernel = kDefaultKernel;  // pitched tile 0..4, strip 5..6, march -1
   std::deque<Request*> queued;
   std::vector<Request*> active;
   std::vector<Request*> retiring;
@@ -234,8 +240,15 @@ int admit(d3d_server s) {
     r->off_a = a;
     r->off_b = b;
     if (s->kernel >= 0) {
-      const int bxm = d3d::pitched_box_x(s->kernel);
-      const int bym = d3d::pitched_box_y(s->kernel);
+      int bxm, bym;
+      if (strip_nr(s->kernel)) {
+        r->strip = d3d::strip_shape(r->px, r->ny, strip_nr(s->kernel));
+        bxm = 4 * r->strip.segs + 8;
+        bym = r->strip.rows + 2;
+      } else {
+        bxm = d3d::pitched_box_x(s->kernel);
+        bym = d3d::pitched_box_y(s->kernel);
+      }
       for (int m = 0; m < 2; ++m) {
         cudaError_t e = d3d::encode_field_map(
             &r->map[m], s->arena + (m ? b : a), r->px, r->ny, r->nz,
@@ -340,16 +353,27 @@ int advance(d3d_server s) {
   }
   std::vector<Request*>& act = s->active;
   const bool pitched = s->kernel >= 0;
+  const int nr = strip_nr(s->kernel);
   int bx = d3d::kBShapes[0].bx, by = d3d::kBShapes[0].by;
-  if (pitched) {
+  if (pitched && !nr) {
     bx = 4 * d3d::pitched_variant(s->kernel).lanes;
     by = d3d::pitched_variant(s->kernel).by;
   }
+  // xy work items of a solve: tiles_x across, tiles_xy in all.
+  auto xy_tiles = [&](const Request* r, int* tx) {
+    if (nr) {
+      *tx = r->strip.pieces;
+      return r->strip.pieces * ((r->ny + r->strip.rows - 1) / r->strip.rows);
+    }
+    *tx = (r->nx + bx - 1) / bx;
+    return *tx * ((r->ny + by - 1) / by);
+  };
   size_t nitems = 0;
   for (int cap = kMaxSlab;; cap /= 2) {
     nitems = 0;
     for (Request* r : act) {
-      const int txy = ((r->nx + bx - 1) / bx) * ((r->ny + by - 1) / by);
+      int tx;
+      const int txy = xy_tiles(r, &tx);
       r->zc = slab_planes(r->nz, cap);
       r->tiles = txy * ((r->nz + r->zc - 1) / r->zc);
       nitems += r->tiles;
@@ -385,8 +409,8 @@ int advance(d3d_server s) {
     }
     float* cur = s->arena + (r->cur_a ? r->off_a : r->off_b);
     float* nxt = s->arena + (r->cur_a ? r->off_b : r->off_a);
-    const int tiles_x = (r->nx + bx - 1) / bx;
-    const int tiles_xy = tiles_x * ((r->ny + by - 1) / by);
+    int tiles_x;
+    const int tiles_xy = xy_tiles(r, &tiles_x);
     if (pitched) {
       d3d::PitchedDesc& d = static_cast<d3d::PitchedDesc*>(st.h_desc)[i];
       d.map[0] = r->map[r->cur_a ? 0 : 1];
@@ -401,6 +425,8 @@ int advance(d3d_server s) {
       d.tiles_xy = tiles_xy;
       d.zc = r->zc;
       d.unused = 0;
+      d.seg_w = r->strip.segs;
+      d.rows = r->strip.rows;
       for (int j = 0; j < 7; ++j) d.k[j] = r->coeff[j];
       d.k[7] = -0.0f;
     } else {
@@ -442,11 +468,14 @@ int advance(d3d_server s) {
     S_TRY(cudaEventRecord(st.start[l], ls), "cudaEventRecord");
     const int* act_l = active_at.data() + (size_t)l * s->chunk;
     for (int j = 0; j < s->chunk && act_l[j] > 0; ++j) {
-      S_TRY(pitched
+      auto* pd = static_cast<d3d::PitchedDesc*>(st.d_desc);
+      S_TRY(nr ? d3d::launch_pitched_strip(nr, pd, st.d_items + item0[l],
+                                           act_l[j], j & 1, ls,
+                                           d3d::device_error_word())
+            : pitched
                 ? d3d::launch_pitched_step(
-                      s->kernel, static_cast<d3d::PitchedDesc*>(st.d_desc),
-                      st.d_items + item0[l], act_l[j], j & 1, ls,
-                      d3d::device_error_word())
+                      s->kernel, pd, st.d_items + item0[l], act_l[j], j & 1,
+                      ls, d3d::device_error_word())
                 : d3d::launch_batch_step(
                       0, static_cast<d3d::BatchDesc*>(st.d_desc),
                       st.d_items + item0[l], act_l[j], j & 1, ls),
@@ -570,7 +599,7 @@ int d3d_server_tick(d3d_server s, long long* done_ids, int max_done,
 
 int d3d_server_set_kernel(d3d_server s, int kernel) {
   if (!s) return sfail(D3D_E_INVALID, "NULL server");
-  if (kernel < -1 || kernel >= d3d::kNumPitchedVariants)
+  if (kernel < -1 || kernel > kMaxKernel)
     return sfail(D3D_E_INVALID, "no such server kernel");
   if (!s->queued.empty() || !s->active.empty() || !s->retiring.empty())
     return sfail(D3D_E_BUSY, "the step kernel changes only on an idle server");

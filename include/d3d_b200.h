@@ -302,7 +302,9 @@ int d3d_server_tick(d3d_server server, long long* done_ids, int max_done,
 
 /* The step kernel of an idle server (D3D_E_BUSY otherwise): 0..4 the
  * pitched TMA kernel's tile shapes (0: 64 x 16, 1: 128 x 16, 2: 128 x 32,
- * 3: 64 x 32 (default), 4: 128 x 8), -1 the batch API's march kernel.
+ * 3: 64 x 32, 4: 128 x 8); 5 and 6 its strip form, where a CTA covers
+ * whole rows of up to 248 columns and a thread takes 1 or 2 16-byte
+ * segments (6 is the default); -1 the batch API's march kernel.
  * With the TMA kernel each solve is stored with rows padded to a multiple
  * of 4 floats, so it takes 2 * ceil4(nx)*ny*nz floats of the arena. */
 int d3d_server_set_kernel(d3d_server server, int kernel);

@@ -59,15 +59,18 @@ def test_same_alone_and_in_the_mix():
 
 
 @pytest.mark.parametrize("kernel,lanes", [(-1, 1), (-1, 2), (0, 3), (1, 1),
-                                          (1, 2), (2, 4), (3, 2), (4, 1)])
+                                          (1, 2), (2, 4), (3, 2), (4, 1),
+                                          (5, 1), (5, 4), (6, 2)])
 def test_every_step_kernel_bit_exact(kernel, lanes):
-    """Each tile shape of the pitched TMA kernel and the march kernel, on
-    1 to 4 compute streams, on grids whose nx leaves 0..3 pad columns
-    (nx = 1 included), single rows and planes, and grids deeper than one z
-    slab."""
+    """Each tile shape of the pitched TMA kernel, its strip forms (5, 6)
+    and the march kernel, on 1 to 4 compute streams, on grids whose nx
+    leaves 0..3 pad columns (nx = 1 included), rows split into several
+    strip pieces (nx > 248), single rows and planes, and grids deeper than
+    one z slab."""
     dims = [(1, 1, 1), (1, 7, 5), (2, 3, 40), (3, 1, 9), (5, 33, 17),
             (8, 8, 8), (13, 17, 19), (64, 16, 3), (130, 9, 35),
-            (131, 70, 6), (257, 5, 4), (36, 35, 70)]
+            (131, 70, 6), (257, 5, 4), (36, 35, 70), (249, 11, 3),
+            (500, 7, 2)]
     reqs = []
     for i, (nx, ny, nz) in enumerate(dims):
         c = B.batch_coefficients(nx, ny, nz, 0.05 + 0.01 * i)
@@ -99,7 +102,7 @@ def test_kernel_and_lanes_change_only_when_idle():
         with pytest.raises(B.D3DError):
             server.set_lanes(bad)
     with pytest.raises(B.D3DError):
-        server.set_kernel(5)
+        server.set_kernel(7)
     server.close()
 
 
