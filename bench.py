@@ -197,7 +197,10 @@ def batched_leg(B, torch, n_grids=4096, plain_sample=64):
     return {"grids": n_grids, "updates": updates, "ms": ms,
             "solves_per_s": solves, "value": updates / (ms / 1e3) / 1e9,
             "unit": UNIT, "launches_per_run": info["launches_per_run"],
-            "tiles": [c["tile"] for c in info["classes"]],
+            "class_kernels": [
+                c["kernel"] + (" %dx%d" % tuple(c["tile"]) if "tile" in c
+                               else " x%d" % c["segments_per_thread"])
+                for c in info["classes"]],
             "plain_loop": {"sample_grids": len(sample),
                            "solves_per_s": plain_solves,
                            "value": upd_s / t_plain / 1e9},

@@ -73,6 +73,7 @@ _SIGNATURES = {
     "d3d_batch_layout": ([_vp, _i, ctypes.POINTER(ctypes.c_size_t)], _i),
     "d3d_batch_create": ([_vp, _i, _vp, _sz, _vpp], _i),
     "d3d_batch_autotune": ([_vp, _vp], _i),
+    "d3d_batch_set_kind": ([_vp, _i], _i),
     "d3d_batch_run": ([_vp, _vp, ctypes.POINTER(ctypes.c_float)], _i),
     "d3d_batch_info": ([_vp, ctypes.c_char_p, _sz], _i),
     "d3d_batch_destroy": ([_vp], _i),
@@ -442,6 +443,11 @@ class Batch:
 
     def autotune(self, stream=None):
         check(lib().d3d_batch_autotune(self._h, _stream_handle(stream)))
+
+    def set_kind(self, kind):
+        """Every size class to one kernel kind: 0..3 the march kernel's
+        tile shapes, 4 and 5 the strip kernel (4 is the default)."""
+        check(lib().d3d_batch_set_kind(self._h, int(kind)))
 
     def run(self, stream=None, timed=True):
         ms = ctypes.c_float()

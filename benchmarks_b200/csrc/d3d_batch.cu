@@ -7,15 +7,21 @@
 // replayed as a single graph launch.
 //
 // Work list.  Grids are split into size classes by nx; each class has one
-// tile shape (BX x BY, 256 threads), picked by the autotuner.  Within a
+// kernel kind, picked by the autotuner from six: the march kernel below
+// with one of four tile shapes (BX x BY, 256 threads) on the caller's dense
+// fields, or the strip form of the pitched TMA kernel (d3d_pitched.cu, 1 or
+// 2 row segments a thread) on pitched copies of the fields.  Within a
 // class, grids are sorted by step count (descending) and every grid
-// contributes one work item per xy tile, so the items still active at step
-// s are a prefix of the class's list: step s launches exactly that prefix.
+// contributes one work item per xy tile (or strip), so the items still
+// active at step s are a prefix of the class's list: step s launches
+// exactly that prefix.  Pitched copies are filled from the caller's inputs
+// at the start of the graph and the results written back at its end, one
+// multi-grid repitch launch each way.
 //
-// Tile kernel: d3d::march_tile (d3d_march.cuh) over one z slab of the
+// March kernel: d3d::march_tile (d3d_march.cuh) over one z slab of the
 // item's grid (the batch API uses one slab of all nz planes; the solve
-// server cuts large grids into several).  Each point is d3d::point: results
-// are bit-identical to running each grid alone.
+// server's march option cuts large grids into several).  Each point is
+// d3d::point: results are bit-identical to running each grid alone.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -85,8 +91,9 @@ namespace {
 using d3d::BatchDesc;
 using d3d::kBShapes;
 using d3d::kNumBShapes;
+using d3d::PitchedDesc;
 
-// Size classes by nx; the autotuner picks one tile shape per class.
+// Size classes by nx; the autotuner picks one kernel kind per class.
 constexpr int kNumClasses = 4;
 int class_of(int nx) {
   if (nx <= 24) return 0;
@@ -95,12 +102,20 @@ int class_of(int nx) {
   return 3;
 }
 
+// Kernel kinds: 0..3 the march kernel's tile shapes (kBShapes) on the
+// caller's dense fields; 4 and 5 the strip form of the pitched TMA kernel
+// (1 or 2 segments a thread) on the batch's pitched copies.
+constexpr int kStripKind = kNumBShapes;
+constexpr int kNumKinds = kNumBShapes + 2;
+constexpr int kDefaultKind = kStripKind;  // before the autotuner runs
+int kind_nr(int kind) { return kind >= kStripKind ? kind - kStripKind + 1 : 0; }
+
 struct ClassPlan {
   std::vector<int> grids;  // batch indices, sorted by steps descending
-  int shape = 0;
+  int kind = 0;
   int max_steps = 0;
   std::vector<int> active;  // items active at step s
-  BatchDesc* d_descs = nullptr;
+  void* d_descs = nullptr;  // BatchDesc or PitchedDesc, by kind
   int2* d_items = nullptr;
   int nitems = 0;
 };
@@ -113,6 +128,13 @@ struct d3d_batch_s {
   size_t arena_bytes = 0;
   int max_steps = 0;
   ClassPlan cls[kNumClasses];
+  // Pitched copies (rows of ceil4(nx) floats) for strip-kind classes, and
+  // the repitch lists that move those grids' inputs in and results out.
+  float* pitched = nullptr;
+  std::vector<unsigned long long> poff;  // per grid: pitched a; b follows
+  d3d::RepitchDesc* d_rep_in = nullptr;
+  d3d::RepitchDesc* d_rep_out = nullptr;
+  int n_rep = 0;
   cudaGraphExec_t exec = nullptr;
   cudaStream_t capture_stream = nullptr;
   cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -135,7 +157,16 @@ int bcuda(cudaError_t e, const char* what) {
     if (e__ != cudaSuccess) return bcuda(e__, what); \
   } while (0)
 
-// (Re)builds one class's descriptors and item list for its current shape.
+int pitch_of(int nx) { return (nx + 3) / 4 * 4; }
+unsigned long long pitched_elems(const d3d_batch_grid& g) {
+  const unsigned long long e = (unsigned long long)pitch_of(g.nx) * g.ny * g.nz;
+  return (e + 63) / 64 * 64;  // 256-byte aligned buffers
+}
+float* pitched_buf(d3d_batch b, int gi, int which) {
+  return b->pitched + b->poff[gi] + (which ? pitched_elems(b->grids[gi]) : 0);
+}
+
+// (Re)builds one class's descriptors and item list for its current kind.
 int build_class(d3d_batch b, ClassPlan& c) {
   if (c.d_descs) cudaFree(c.d_descs);
   if (c.d_items) cudaFree(c.d_items);
@@ -144,40 +175,119 @@ int build_class(d3d_batch b, ClassPlan& c) {
   c.active.assign(c.max_steps, 0);
   c.nitems = 0;
   if (c.grids.empty()) return D3D_OK;
-  const d3d::BShape sh = kBShapes[c.shape];
+  const int nr = kind_nr(c.kind);
   std::vector<BatchDesc> descs;
+  std::vector<PitchedDesc> pdescs;
   std::vector<int2> items;
   for (size_t gi = 0; gi < c.grids.size(); ++gi) {
-    const d3d_batch_grid& g = b->grids[c.grids[gi]];
-    BatchDesc d;
-    d.a = b->arena + g.offset_a;
-    d.b = b->arena + g.offset_b;
-    d.nx = g.nx;
-    d.ny = g.ny;
-    d.nz = g.nz;
-    d.tiles_x = (g.nx + sh.bx - 1) / sh.bx;
-    const int tiles = d.tiles_x * ((g.ny + sh.by - 1) / sh.by);
-    d.tiles_xy = tiles;
-    d.zc = g.nz;  // one slab: batches bring parallelism in grid count
-    for (int j = 0; j < 7; ++j) d.k[j] = g.coeff[j];
-    d.k[7] = -0.0f;
-    descs.push_back(d);
+    const int id = c.grids[gi];
+    const d3d_batch_grid& g = b->grids[id];
+    int tiles;
+    if (nr) {
+      const int px = pitch_of(g.nx);
+      const d3d::StripShape sh = d3d::strip_shape(px, g.ny, nr);
+      PitchedDesc d;
+      memset(&d, 0, sizeof d);
+      d.a = pitched_buf(b, id, 0);
+      d.b = pitched_buf(b, id, 1);
+      for (int m = 0; m < 2; ++m) {
+        cudaError_t e = d3d::encode_field_map(
+            &d.map[m], m ? d.b : d.a, px, g.ny, g.nz, d3d::kF32,
+            4 * sh.segs + 8, sh.rows + 2);
+        if (e != cudaSuccess) return bcuda(e, "tensor map of a batch grid");
+      }
+      d.nx = g.nx;
+      d.px = px;
+      d.ny = g.ny;
+      d.nz = g.nz;
+      d.tiles_x = sh.pieces;
+      d.tiles_xy = sh.pieces * ((g.ny + sh.rows - 1) / sh.rows);
+      d.zc = g.nz;  // one slab: batches bring parallelism in grid count
+      d.seg_w = sh.segs;
+      d.rows = sh.rows;
+      for (int j = 0; j < 7; ++j) d.k[j] = g.coeff[j];
+      d.k[7] = -0.0f;
+      tiles = d.tiles_xy;
+      pdescs.push_back(d);
+    } else {
+      const d3d::BShape sh = kBShapes[c.kind];
+      BatchDesc d;
+      d.a = b->arena + g.offset_a;
+      d.b = b->arena + g.offset_b;
+      d.nx = g.nx;
+      d.ny = g.ny;
+      d.nz = g.nz;
+      d.tiles_x = (g.nx + sh.bx - 1) / sh.bx;
+      d.tiles_xy = d.tiles_x * ((g.ny + sh.by - 1) / sh.by);
+      d.zc = g.nz;
+      for (int j = 0; j < 7; ++j) d.k[j] = g.coeff[j];
+      d.k[7] = -0.0f;
+      tiles = d.tiles_xy;
+      descs.push_back(d);
+    }
     for (int t = 0; t < tiles; ++t) items.push_back(make_int2((int)gi, t));
     // items of this grid are active for steps [0, g.steps)
-    for (int s = 0; s < g.steps; ++s) c.active[s] += tiles;
+    for (int st = 0; st < g.steps; ++st) c.active[st] += tiles;
   }
   c.nitems = (int)items.size();
-  B_TRY(cudaMalloc(&c.d_descs, descs.size() * sizeof(BatchDesc)),
-        "cudaMalloc (batch descriptors)");
+  const size_t dbytes = nr ? pdescs.size() * sizeof(PitchedDesc)
+                           : descs.size() * sizeof(BatchDesc);
+  B_TRY(cudaMalloc(&c.d_descs, dbytes), "cudaMalloc (batch descriptors)");
   B_TRY(cudaMalloc(&c.d_items, items.size() * sizeof(int2)),
         "cudaMalloc (batch items)");
-  B_TRY(cudaMemcpy(c.d_descs, descs.data(), descs.size() * sizeof(BatchDesc),
-                   cudaMemcpyHostToDevice),
+  B_TRY(cudaMemcpy(c.d_descs,
+                   nr ? static_cast<const void*>(pdescs.data())
+                      : static_cast<const void*>(descs.data()),
+                   dbytes, cudaMemcpyHostToDevice),
         "H2D descriptors");
   B_TRY(cudaMemcpy(c.d_items, items.data(), items.size() * sizeof(int2),
                    cudaMemcpyHostToDevice),
         "H2D items");
   return D3D_OK;
+}
+
+// The repitch lists of every grid (steps > 0) in a strip-kind class.
+int build_repitch(d3d_batch b) {
+  if (b->d_rep_in) cudaFree(b->d_rep_in);
+  if (b->d_rep_out) cudaFree(b->d_rep_out);
+  b->d_rep_in = b->d_rep_out = nullptr;
+  b->n_rep = 0;
+  std::vector<d3d::RepitchDesc> in, out;
+  for (const ClassPlan& c : b->cls) {
+    if (!kind_nr(c.kind)) continue;
+    for (int id : c.grids) {
+      const d3d_batch_grid& g = b->grids[id];
+      if (g.steps == 0) continue;  // its result is its input
+      const long long rows = (long long)g.ny * g.nz;
+      in.push_back({b->arena + g.offset_a, pitched_buf(b, id, 0), g.nx,
+                    pitch_of(g.nx), rows});
+      out.push_back({b->arena + ((g.steps & 1) ? g.offset_b : g.offset_a),
+                     pitched_buf(b, id, g.steps & 1), g.nx, pitch_of(g.nx),
+                     rows});
+    }
+  }
+  if (in.empty()) return D3D_OK;
+  const size_t bytes = in.size() * sizeof(d3d::RepitchDesc);
+  B_TRY(cudaMalloc(&b->d_rep_in, bytes), "cudaMalloc (repitch lists)");
+  B_TRY(cudaMalloc(&b->d_rep_out, bytes), "cudaMalloc (repitch lists)");
+  B_TRY(cudaMemcpy(b->d_rep_in, in.data(), bytes, cudaMemcpyHostToDevice),
+        "H2D repitch lists");
+  B_TRY(cudaMemcpy(b->d_rep_out, out.data(), bytes, cudaMemcpyHostToDevice),
+        "H2D repitch lists");
+  b->n_rep = (int)in.size();
+  return D3D_OK;
+}
+
+cudaError_t launch_class_step(const ClassPlan& c, int nitems, int parity,
+                              cudaStream_t s) {
+  const int nr = kind_nr(c.kind);
+  if (nr)
+    return d3d::launch_pitched_strip(
+        nr, static_cast<const PitchedDesc*>(c.d_descs), c.d_items, nitems,
+        parity, s, d3d::device_error_word());
+  return d3d::launch_batch_step(c.kind,
+                                static_cast<const BatchDesc*>(c.d_descs),
+                                c.d_items, nitems, parity, s);
 }
 
 // All steps of all classes, in step order (class launches of one step are
@@ -190,8 +300,7 @@ int enqueue_run(d3d_batch b, cudaStream_t s, int only_class, int max_steps,
       if (only_class >= 0 && ci != only_class) continue;
       ClassPlan& c = b->cls[ci];
       if (step >= c.max_steps || c.active[step] == 0) continue;
-      B_TRY(d3d::launch_batch_step(c.shape, c.d_descs, c.d_items,
-                                   c.active[step], step & 1, s),
+      B_TRY(launch_class_step(c, c.active[step], step & 1, s),
             "batch step launch");
       ++n;
     }
@@ -267,6 +376,18 @@ int d3d_batch_create(const d3d_batch_grid* grids, int n, void* arena,
   b->arena = static_cast<float*>(arena);
   b->arena_bytes = arena_bytes;
   cudaGetDevice(&b->device);
+  // Pitched copies for the strip kinds, two buffers per grid.
+  b->poff.resize(n);
+  unsigned long long pe = 0;
+  for (int i = 0; i < n; ++i) {
+    b->poff[i] = pe;
+    pe += 2 * pitched_elems(grids[i]);
+  }
+  if (cudaMalloc(&b->pitched, pe * sizeof(float)) != cudaSuccess) {
+    cudaGetLastError();
+    d3d_batch_destroy(b);
+    return bfail(D3D_E_OOM, "pitched copies of the batch");
+  }
   for (int i = 0; i < n; ++i) {
     ClassPlan& c = b->cls[class_of(grids[i].nx)];
     c.grids.push_back(i);
@@ -277,13 +398,18 @@ int d3d_batch_create(const d3d_batch_grid* grids, int n, void* arena,
     std::stable_sort(c.grids.begin(), c.grids.end(), [&](int x, int y) {
       return b->grids[x].steps > b->grids[y].steps;
     });
-    c.shape = 0;
+    c.kind = kDefaultKind;
     int rc = build_class(b, c);
     if (rc) {
       d3d_batch_destroy(b);
       return rc;
     }
-    for (int s = 0; s < c.max_steps; ++s) b->total_items += c.active[s];
+    for (int st = 0; st < c.max_steps; ++st) b->total_items += c.active[st];
+  }
+  int rc = build_repitch(b);
+  if (rc) {
+    d3d_batch_destroy(b);
+    return rc;
   }
   if (cudaEventCreate(&b->ev[0]) != cudaSuccess ||
       cudaEventCreate(&b->ev[1]) != cudaSuccess) {
@@ -298,15 +424,16 @@ int d3d_batch_autotune(d3d_batch b, void* stream) {
   if (!b) return bfail(D3D_E_INVALID, "NULL batch");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   drop_graph(b);
+  b->total_items = 0;
   for (int ci = 0; ci < kNumClasses; ++ci) {
     ClassPlan& c = b->cls[ci];
     if (c.grids.empty()) continue;
     const int probe_steps = std::min(c.max_steps, 8);
     if (probe_steps == 0) continue;
     float best = -1.0f;
-    int best_shape = c.shape;
-    for (int sh = 0; sh < kNumBShapes; ++sh) {
-      c.shape = sh;
+    int best_kind = c.kind;
+    for (int kind = 0; kind < kNumKinds; ++kind) {
+      c.kind = kind;
       int rc = build_class(b, c);
       if (rc) return rc;
       rc = enqueue_run(b, s, ci, 1, nullptr);  // warm-up
@@ -320,14 +447,31 @@ int d3d_batch_autotune(d3d_batch b, void* stream) {
       B_TRY(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]), "elapsed");
       if (best < 0.0f || ms < best) {
         best = ms;
-        best_shape = sh;
+        best_kind = kind;
       }
     }
-    c.shape = best_shape;
+    c.kind = best_kind;
     int rc = build_class(b, c);
     if (rc) return rc;
   }
-  return D3D_OK;
+  for (const ClassPlan& c : b->cls)
+    for (int st = 0; st < c.max_steps; ++st) b->total_items += c.active[st];
+  return build_repitch(b);
+}
+
+int d3d_batch_set_kind(d3d_batch b, int kind) {
+  if (!b) return bfail(D3D_E_INVALID, "NULL batch");
+  if (kind < 0 || kind >= kNumKinds)
+    return bfail(D3D_E_INVALID, "no such kernel kind");
+  drop_graph(b);
+  b->total_items = 0;
+  for (ClassPlan& c : b->cls) {
+    c.kind = kind;
+    int rc = build_class(b, c);
+    if (rc) return rc;
+    for (int st = 0; st < c.max_steps; ++st) b->total_items += c.active[st];
+  }
+  return build_repitch(b);
 }
 
 int d3d_batch_run(d3d_batch b, void* stream, float* kernel_ms) {
@@ -344,10 +488,21 @@ int d3d_batch_run(d3d_batch b, void* stream, float* kernel_ms) {
     B_TRY(cudaStreamBeginCapture(b->capture_stream,
                                  cudaStreamCaptureModeThreadLocal),
           "cudaStreamBeginCapture");
-    int rc = enqueue_run(b, b->capture_stream, -1, b->max_steps,
-                         &b->launches_per_run);
+    // Strip-kind grids: inputs into the pitched copies, the steps, results
+    // back into the caller's arena.
+    unsigned long long steps_launched = 0;
+    cudaError_t e = d3d::launch_repitch_multi(b->d_rep_in, b->n_rep, true,
+                                              b->capture_stream);
+    int rc = e == cudaSuccess ? enqueue_run(b, b->capture_stream, -1,
+                                            b->max_steps, &steps_launched)
+                              : bcuda(e, "repitch launch");
+    if (!rc) {
+      e = d3d::launch_repitch_multi(b->d_rep_out, b->n_rep, false,
+                                    b->capture_stream);
+      if (e != cudaSuccess) rc = bcuda(e, "repitch launch");
+    }
     cudaGraph_t g = nullptr;
-    cudaError_t e = cudaStreamEndCapture(b->capture_stream, &g);
+    e = cudaStreamEndCapture(b->capture_stream, &g);
     if (rc) {
       if (g) cudaGraphDestroy(g);
       return rc;
@@ -359,6 +514,7 @@ int d3d_batch_run(d3d_batch b, void* stream, float* kernel_ms) {
       b->exec = nullptr;
       return bcuda(e, "cudaGraphInstantiate");
     }
+    b->launches_per_run = steps_launched + (b->n_rep ? 2 : 0);
   }
   B_TRY(cudaEventRecord(b->ev[0], s), "cudaEventRecord");
   B_TRY(cudaGraphLaunch(b->exec, s), "cudaGraphLaunch");
@@ -380,10 +536,18 @@ int d3d_batch_info(d3d_batch b, char* buf, size_t len) {
                       b->launches_per_run);
   for (int ci = 0; ci < kNumClasses && used < (int)len; ++ci) {
     const ClassPlan& c = b->cls[ci];
-    used += snprintf(buf + used, len - used,
-                     "%s{\"grids\": %zu, \"tile\": [%d, %d], \"items\": %d}",
-                     ci ? ", " : "", c.grids.size(), kBShapes[c.shape].bx,
-                     kBShapes[c.shape].by, c.nitems);
+    const int nr = kind_nr(c.kind);
+    if (nr)
+      used += snprintf(buf + used, len - used,
+                       "%s{\"grids\": %zu, \"kernel\": \"strip\", "
+                       "\"segments_per_thread\": %d, \"items\": %d}",
+                       ci ? ", " : "", c.grids.size(), nr, c.nitems);
+    else
+      used += snprintf(buf + used, len - used,
+                       "%s{\"grids\": %zu, \"kernel\": \"march\", "
+                       "\"tile\": [%d, %d], \"items\": %d}",
+                       ci ? ", " : "", c.grids.size(), kBShapes[c.kind].bx,
+                       kBShapes[c.kind].by, c.nitems);
   }
   if (used < (int)len) snprintf(buf + used, len - used, "]}");
   return D3D_OK;
@@ -396,6 +560,9 @@ int d3d_batch_destroy(d3d_batch b) {
     if (c.d_descs) cudaFree(c.d_descs);
     if (c.d_items) cudaFree(c.d_items);
   }
+  if (b->d_rep_in) cudaFree(b->d_rep_in);
+  if (b->d_rep_out) cudaFree(b->d_rep_out);
+  if (b->pitched) cudaFree(b->pitched);
   if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
   if (b->ev[0]) cudaEventDestroy(b->ev[0]);
   if (b->ev[1]) cudaEventDestroy(b->ev[1]);

@@ -173,6 +173,19 @@ cudaError_t launch_pitched_strip(int nr, const PitchedDesc* descs,
                                  const int2* items, int nitems, int parity,
                                  cudaStream_t s, unsigned* dev_err);
 
+// One grid of a multi-grid repitch: `rows` (= ny * nz) rows of nx floats
+// at `dense`, px floats at `pitched`.
+struct RepitchDesc {
+  float* dense;
+  float* pitched;
+  int nx, px;
+  long long rows;
+};
+// Dense -> pitched (pads filled from column nx-1) when to_pitched, else
+// pitched -> dense, for n grids in one launch.
+cudaError_t launch_repitch_multi(const RepitchDesc* d, int n,
+                                 bool to_pitched, cudaStream_t s);
+
 // Dense rows (nx floats) -> pitched rows (px floats, pads filled from
 // column nx-1) when to_pitched, else pitched -> dense; rows = ny * nz.
 // src and dst must not overlap.

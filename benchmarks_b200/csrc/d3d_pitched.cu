@@ -491,6 +491,36 @@ cudaError_t launch_pitched_step(int variant, const PitchedDesc* descs,
   }
 }
 
+// Many grids' repitch in one launch: block row blockIdx.y takes grids
+// blockIdx.y, blockIdx.y + gridDim.y, ...; blockIdx.x strides their rows.
+__global__ void __launch_bounds__(128)
+    repitch_multi_kernel(const RepitchDesc* __restrict__ d, int n,
+                         bool to_pitched) {
+  for (int g = blockIdx.y; g < n; g += gridDim.y) {
+    const RepitchDesc r = d[g];
+    for (long long row = blockIdx.x; row < r.rows; row += gridDim.x) {
+      if (to_pitched) {
+        const float* in = r.dense + (size_t)row * r.nx;
+        float* out = r.pitched + (size_t)row * r.px;
+        for (int x = threadIdx.x; x < r.px; x += blockDim.x)
+          out[x] = in[min(x, r.nx - 1)];
+      } else {
+        const float* in = r.pitched + (size_t)row * r.px;
+        float* out = r.dense + (size_t)row * r.nx;
+        for (int x = threadIdx.x; x < r.nx; x += blockDim.x) out[x] = in[x];
+      }
+    }
+  }
+}
+
+cudaError_t launch_repitch_multi(const RepitchDesc* d, int n,
+                                 bool to_pitched, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const dim3 grid(8, (unsigned)std::min(n, 65535));
+  repitch_multi_kernel<<<grid, 128, 0, s>>>(d, n, to_pitched);
+  return cudaGetLastError();
+}
+
 StripShape strip_shape(int px, int ny, int nr) {
   StripShape sh;
   sh.pieces = (px + kStripMaxW - 1) / kStripMaxW;

@@ -208,8 +208,11 @@ int d3d_compare(d3d_plan plan, const void* a, int a_dtype, const void* b,
 /* ---------------------------------------------------------------------
  * Batched solves: many independent FP32 grids of different shapes,
  * coefficients and step counts advanced together -- one multi-grid step
- * kernel per size class and time step, the whole run captured once into a
- * CUDA graph and replayed as one graph launch.  No counterpart in the
+ * launch per size class and time step, the whole run captured once into a
+ * CUDA graph and replayed as one graph launch.  Each size class runs the
+ * kernel its autotuner picked: a shared-memory march over the caller's
+ * fields, or a TMA strip kernel over pitched copies the batch keeps (and
+ * fills and writes back inside the same graph).  No counterpart in the
  * reference (which runs one grid per
  * process); each grid's arithmetic is still RunKernel's, so every grid's
  * result is bit-identical to running it alone (with the reference or with
@@ -240,24 +243,32 @@ int d3d_batch_coefficients(int nx, int ny, int nz, float kappa,
  * their offsets; *arena_bytes receives the arena size needed. */
 int d3d_batch_layout(d3d_batch_grid* grids, int n, size_t* arena_bytes);
 
-/* Builds the batch: descriptors, size classes, and the work queue (grids
- * ordered by step count and packed into waves whose fields fit in L2).
+/* Builds the batch: size classes by nx, each class's grids ordered by step
+ * count, their descriptors and work items, and device memory for pitched
+ * copies of every grid (two buffers of ceil4(nx)*ny*nz floats each).
  * `arena` must stay valid for the batch's lifetime. */
 int d3d_batch_create(const d3d_batch_grid* grids, int n, void* arena,
                      size_t arena_bytes, d3d_batch* out);
 
-/* Times each tile shape per size class on the batch's own grids (their
- * fields are overwritten) and keeps the fastest per class. */
+/* Times each kernel kind (4 march tile shapes, 2 strip forms) per size
+ * class on the batch's own grids (their fields are overwritten) and keeps
+ * the fastest per class. */
 int d3d_batch_autotune(d3d_batch batch, void* stream);
 
-/* Runs every grid for its step count: one cooperative persistent launch
- * (replayed from a CUDA graph after the first run).  *kernel_ms (may be
- * NULL) receives the device time.  Returns D3D_E_TIMEOUT if a bounded
- * inter-CTA wait ran out (the kernel then exits early; results are
- * invalid). */
+/* Sets every size class to one kernel kind: 0..3 the march kernel with
+ * tile 32x16 (x pairs), 64x8 (x pairs), 32x8, 16x16; 4 and 5 the strip
+ * kernel with 1 or 2 segments a thread (4 is the default before
+ * d3d_batch_autotune). */
+int d3d_batch_set_kind(d3d_batch batch, int kind);
+
+/* Runs every grid for its step count: the first call captures the run
+ * into a CUDA graph, every call replays it as one graph launch.
+ * *kernel_ms (may be NULL) receives the device time.  A bounded wait that
+ * ran out in the TMA kernel is reported by d3d_check_device_errors. */
 int d3d_batch_run(d3d_batch batch, void* stream, float* kernel_ms);
 
-/* JSON summary: grids, waves, work items, tile shape per class, CTAs. */
+/* JSON summary: grids, steps, work items, launches per run, and per size
+ * class its kernel (march tile shape or strip form) and work items. */
 int d3d_batch_info(d3d_batch batch, char* buf, size_t len);
 
 int d3d_batch_destroy(d3d_batch batch);

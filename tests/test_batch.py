@@ -95,11 +95,13 @@ def _fields(specs, seed):
     return out
 
 
-def _run_batch(specs, fields, autotune=False):
+def _run_batch(specs, fields, autotune=False, kind=None):
     torch = pytest.importorskip("torch")
     batch = B.Batch(specs)
     if autotune:
         batch.autotune()
+    if kind is not None:
+        batch.set_kind(kind)
     for i, f in enumerate(fields):
         batch.input(i).copy_(torch.from_numpy(f))
     batch.run()
@@ -142,8 +144,32 @@ def test_autotuned_batch_still_bit_exact():
     outs, batch = _run_batch(specs, fields, autotune=True)
     for (nx, ny, nz, steps, c), f, o in zip(specs, fields, outs):
         assert o.tobytes() == O.run(f, c, steps).tobytes()
-    shapes = {tuple(c["tile"]) for c in batch.info()["classes"]}
-    assert shapes <= {(64, 8), (32, 16), (32, 8), (16, 16)}
+    for c in batch.info()["classes"]:
+        if c["kernel"] == "march":
+            assert tuple(c["tile"]) in {(64, 8), (32, 16), (32, 8), (16, 16)}
+        else:
+            assert c["kernel"] == "strip"
+            assert c["segments_per_thread"] in (1, 2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", range(6))
+def test_every_kernel_kind_bit_exact(kind):
+    """Each march tile shape and both strip forms on grids of every size
+    class, nx leaving 0..3 pad columns in the pitched copies (nx = 1
+    included), zero-step grids, odd and even step counts."""
+    dims = [(1, 1, 1), (1, 5, 7), (3, 2, 9), (17, 23, 5), (24, 9, 13),
+            (25, 30, 2), (40, 41, 11), (41, 3, 6), (72, 17, 8), (73, 70, 9),
+            (96, 96, 4), (13, 1, 30)]
+    specs = [(nx, ny, nz, (i * 5) % 9,
+              B.batch_coefficients(nx, ny, nz, 0.05 + 0.01 * i))
+             for i, (nx, ny, nz) in enumerate(dims)]
+    fields = _fields(specs, 1100 + kind)
+    outs, batch = _run_batch(specs, fields, kind=kind)
+    for (nx, ny, nz, steps, c), f, o in zip(specs, fields, outs):
+        assert o.tobytes() == O.run(f, c, steps).tobytes(), (kind, nx, ny,
+                                                              nz, steps)
+    assert B.check_device_errors() == 0
 
 
 @pytest.mark.gpu
