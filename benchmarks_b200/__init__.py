@@ -446,7 +446,8 @@ class Batch:
 
     def set_kind(self, kind):
         """Every size class to one kernel kind: 0..3 the march kernel's
-        tile shapes, 4 and 5 the strip kernel (4 is the default)."""
+        tile shapes, 4 and 5 the strip kernel (4 is the default), 6 and 7
+        its two-step form (grids at most 248 floats wide)."""
         check(lib().d3d_batch_set_kind(self._h, int(kind)))
 
     def run(self, stream=None, timed=True):

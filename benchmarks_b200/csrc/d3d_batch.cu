@@ -104,20 +104,36 @@ int class_of(int nx) {
 
 // Kernel kinds: 0..3 the march kernel's tile shapes (kBShapes) on the
 // caller's dense fields; 4 and 5 the strip form of the pitched TMA kernel
-// (1 or 2 segments a thread) on the batch's pitched copies.
+// (1 or 2 segments a thread) on the batch's pitched copies; 6 and 7 its
+// two-step form (temporal-block depth 2: fused step pairs, then one strip
+// step for an odd step count), for classes whose grids are at most
+// d3d::kStripMaxW floats wide.
 constexpr int kStripKind = kNumBShapes;
-constexpr int kNumKinds = kNumBShapes + 2;
+constexpr int kStrip2Kind = kStripKind + 2;
+constexpr int kNumKinds = kStrip2Kind + 2;
 constexpr int kDefaultKind = kStripKind;  // before the autotuner runs
-int kind_nr(int kind) { return kind >= kStripKind ? kind - kStripKind + 1 : 0; }
+int kind_nr(int kind) {
+  return kind >= kStrip2Kind ? kind - kStrip2Kind + 1
+         : kind >= kStripKind ? kind - kStripKind + 1
+                              : 0;
+}
+bool kind_two(int kind) { return kind >= kStrip2Kind; }
 
 struct ClassPlan {
   std::vector<int> grids;  // batch indices, sorted by steps descending
   int kind = 0;
   int max_steps = 0;
-  std::vector<int> active;  // items active at step s
+  // Launch j (a step, or for two-step kinds a fused pair) covers the first
+  // active[j] items.
+  std::vector<int> active;
   void* d_descs = nullptr;  // BatchDesc or PitchedDesc, by kind
   int2* d_items = nullptr;
   int nitems = 0;
+  // Two-step kinds: the single strip step of grids with an odd step count,
+  // after pass j: items [one_lo[j], one_lo[j] + one_n[j]) of d_items1.
+  PitchedDesc* d_descs1 = nullptr;
+  int2* d_items1 = nullptr;
+  std::vector<int> one_lo, one_n;
 };
 
 }  // namespace
@@ -166,49 +182,105 @@ float* pitched_buf(d3d_batch b, int gi, int which) {
   return b->pitched + b->poff[gi] + (which ? pitched_elems(b->grids[gi]) : 0);
 }
 
-// (Re)builds one class's descriptors and item list for its current kind.
-int build_class(d3d_batch b, ClassPlan& c) {
+// Whether every grid of a class fits the two-step form.
+bool class_takes_two_step(const d3d_batch b, const ClassPlan& c) {
+  for (int id : c.grids)
+    if (pitch_of(b->grids[id].nx) > d3d::kStripMaxW) return false;
+  return true;
+}
+
+// A strip-form descriptor of grid `id` (boxes of `rows + extra` rows).
+int strip_desc(d3d_batch b, int id, const d3d::StripShape& sh, int extra,
+               PitchedDesc* d) {
+  const d3d_batch_grid& g = b->grids[id];
+  const int px = pitch_of(g.nx);
+  memset(d, 0, sizeof *d);
+  d->a = pitched_buf(b, id, 0);
+  d->b = pitched_buf(b, id, 1);
+  for (int m = 0; m < 2; ++m) {
+    cudaError_t e = d3d::encode_field_map(&d->map[m], m ? d->b : d->a, px,
+                                          g.ny, g.nz, d3d::kF32,
+                                          4 * sh.segs + 8, sh.rows + extra);
+    if (e != cudaSuccess) return bcuda(e, "tensor map of a batch grid");
+  }
+  d->nx = g.nx;
+  d->px = px;
+  d->ny = g.ny;
+  d->nz = g.nz;
+  d->tiles_x = sh.pieces;
+  d->tiles_xy = sh.pieces * ((g.ny + sh.rows - 1) / sh.rows);
+  d->zc = g.nz;  // one slab: batches bring parallelism in grid count
+  d->seg_w = sh.segs;
+  d->rows = sh.rows;
+  for (int j = 0; j < 7; ++j) d->k[j] = g.coeff[j];
+  d->k[7] = -0.0f;
+  return D3D_OK;
+}
+
+template <typename T>
+int upload(const std::vector<T>& v, T** out, const char* what) {
+  *out = nullptr;
+  if (v.empty()) return D3D_OK;
+  B_TRY(cudaMalloc(out, v.size() * sizeof(T)), what);
+  B_TRY(cudaMemcpy(*out, v.data(), v.size() * sizeof(T),
+                   cudaMemcpyHostToDevice),
+        what);
+  return D3D_OK;
+}
+
+void free_class(ClassPlan& c) {
   if (c.d_descs) cudaFree(c.d_descs);
   if (c.d_items) cudaFree(c.d_items);
+  if (c.d_descs1) cudaFree(c.d_descs1);
+  if (c.d_items1) cudaFree(c.d_items1);
   c.d_descs = nullptr;
   c.d_items = nullptr;
-  c.active.assign(c.max_steps, 0);
+  c.d_descs1 = nullptr;
+  c.d_items1 = nullptr;
+}
+
+// (Re)builds one class's descriptors and item lists for its current kind.
+int build_class(d3d_batch b, ClassPlan& c) {
+  free_class(c);
+  const bool two = kind_two(c.kind);
+  const int nr = kind_nr(c.kind);
+  const int nlaunch = two ? c.max_steps / 2 : c.max_steps;
+  c.active.assign(nlaunch, 0);
+  c.one_lo.assign(c.max_steps / 2 + 1, 0);
+  c.one_n.assign(c.max_steps / 2 + 1, 0);
   c.nitems = 0;
   if (c.grids.empty()) return D3D_OK;
-  const int nr = kind_nr(c.kind);
   std::vector<BatchDesc> descs;
-  std::vector<PitchedDesc> pdescs;
-  std::vector<int2> items;
+  std::vector<PitchedDesc> pdescs, pdescs1;
+  std::vector<int2> items, items1;
   for (size_t gi = 0; gi < c.grids.size(); ++gi) {
     const int id = c.grids[gi];
     const d3d_batch_grid& g = b->grids[id];
     int tiles;
-    if (nr) {
+    if (two) {
       const int px = pitch_of(g.nx);
-      const d3d::StripShape sh = d3d::strip_shape(px, g.ny, nr);
-      PitchedDesc d;
-      memset(&d, 0, sizeof d);
-      d.a = pitched_buf(b, id, 0);
-      d.b = pitched_buf(b, id, 1);
-      for (int m = 0; m < 2; ++m) {
-        cudaError_t e = d3d::encode_field_map(
-            &d.map[m], m ? d.b : d.a, px, g.ny, g.nz, d3d::kF32,
-            4 * sh.segs + 8, sh.rows + 2);
-        if (e != cudaSuccess) return bcuda(e, "tensor map of a batch grid");
-      }
-      d.nx = g.nx;
-      d.px = px;
-      d.ny = g.ny;
-      d.nz = g.nz;
-      d.tiles_x = sh.pieces;
-      d.tiles_xy = sh.pieces * ((g.ny + sh.rows - 1) / sh.rows);
-      d.zc = g.nz;  // one slab: batches bring parallelism in grid count
-      d.seg_w = sh.segs;
-      d.rows = sh.rows;
-      for (int j = 0; j < 7; ++j) d.k[j] = g.coeff[j];
-      d.k[7] = -0.0f;
-      tiles = d.tiles_xy;
+      PitchedDesc d, d1;
+      int rc = strip_desc(b, id, d3d::strip2_shape(px, g.ny, nr), 4, &d);
+      if (rc) return rc;
+      rc = strip_desc(b, id, d3d::strip_shape(px, g.ny, 1), 2, &d1);
+      if (rc) return rc;
       pdescs.push_back(d);
+      pdescs1.push_back(d1);
+      tiles = d.tiles_xy;
+      if (g.steps & 1) {
+        const int j = g.steps / 2;
+        if (c.one_n[j] == 0) c.one_lo[j] = (int)items1.size();
+        for (int t = 0; t < d1.tiles_xy; ++t)
+          items1.push_back(make_int2((int)gi, t));
+        c.one_n[j] += d1.tiles_xy;
+      }
+    } else if (nr) {
+      PitchedDesc d;
+      int rc = strip_desc(b, id, d3d::strip_shape(pitch_of(g.nx), g.ny, nr),
+                          2, &d);
+      if (rc) return rc;
+      pdescs.push_back(d);
+      tiles = d.tiles_xy;
     } else {
       const d3d::BShape sh = kBShapes[c.kind];
       BatchDesc d;
@@ -226,24 +298,26 @@ int build_class(d3d_batch b, ClassPlan& c) {
       descs.push_back(d);
     }
     for (int t = 0; t < tiles; ++t) items.push_back(make_int2((int)gi, t));
-    // items of this grid are active for steps [0, g.steps)
-    for (int st = 0; st < g.steps; ++st) c.active[st] += tiles;
+    // this grid's items are in launches [0, steps) (pairs: [0, steps/2))
+    const int nl = two ? g.steps / 2 : g.steps;
+    for (int j = 0; j < nl; ++j) c.active[j] += tiles;
   }
   c.nitems = (int)items.size();
-  const size_t dbytes = nr ? pdescs.size() * sizeof(PitchedDesc)
-                           : descs.size() * sizeof(BatchDesc);
-  B_TRY(cudaMalloc(&c.d_descs, dbytes), "cudaMalloc (batch descriptors)");
-  B_TRY(cudaMalloc(&c.d_items, items.size() * sizeof(int2)),
-        "cudaMalloc (batch items)");
-  B_TRY(cudaMemcpy(c.d_descs,
-                   nr ? static_cast<const void*>(pdescs.data())
-                      : static_cast<const void*>(descs.data()),
-                   dbytes, cudaMemcpyHostToDevice),
-        "H2D descriptors");
-  B_TRY(cudaMemcpy(c.d_items, items.data(), items.size() * sizeof(int2),
-                   cudaMemcpyHostToDevice),
-        "H2D items");
-  return D3D_OK;
+  int rc = nr ? upload(pdescs, reinterpret_cast<PitchedDesc**>(&c.d_descs),
+                       "batch descriptors")
+              : upload(descs, reinterpret_cast<BatchDesc**>(&c.d_descs),
+                       "batch descriptors");
+  if (!rc) rc = upload(items, &c.d_items, "batch items");
+  if (!rc) rc = upload(pdescs1, &c.d_descs1, "batch descriptors");
+  if (!rc) rc = upload(items1, &c.d_items1, "batch items");
+  return rc;
+}
+
+// The pitched buffer (0: a, 1: b) holding grid `g`'s result under a kind:
+// one step swaps the buffers, a fused pair swaps them once.
+int result_buffer(const d3d_batch_grid& g, int kind) {
+  const int swaps = kind_two(kind) ? g.steps / 2 + (g.steps & 1) : g.steps;
+  return swaps & 1;
 }
 
 // The repitch lists of every grid (steps > 0) in a strip-kind class.
@@ -262,8 +336,8 @@ int build_repitch(d3d_batch b) {
       in.push_back({b->arena + g.offset_a, pitched_buf(b, id, 0), g.nx,
                     pitch_of(g.nx), rows});
       out.push_back({b->arena + ((g.steps & 1) ? g.offset_b : g.offset_a),
-                     pitched_buf(b, id, g.steps & 1), g.nx, pitch_of(g.nx),
-                     rows});
+                     pitched_buf(b, id, result_buffer(g, c.kind)), g.nx,
+                     pitch_of(g.nx), rows});
     }
   }
   if (in.empty()) return D3D_OK;
@@ -281,6 +355,10 @@ int build_repitch(d3d_batch b) {
 cudaError_t launch_class_step(const ClassPlan& c, int nitems, int parity,
                               cudaStream_t s) {
   const int nr = kind_nr(c.kind);
+  if (kind_two(c.kind))
+    return d3d::launch_pitched_strip2(
+        nr, static_cast<const PitchedDesc*>(c.d_descs), c.d_items, nitems,
+        parity, s, d3d::device_error_word());
   if (nr)
     return d3d::launch_pitched_strip(
         nr, static_cast<const PitchedDesc*>(c.d_descs), c.d_items, nitems,
@@ -299,7 +377,27 @@ int enqueue_run(d3d_batch b, cudaStream_t s, int only_class, int max_steps,
     for (int ci = 0; ci < kNumClasses; ++ci) {
       if (only_class >= 0 && ci != only_class) continue;
       ClassPlan& c = b->cls[ci];
-      if (step >= c.max_steps || c.active[step] == 0) continue;
+      if (step >= c.max_steps) continue;
+      if (kind_two(c.kind)) {
+        // Pair j = step / 2 at even steps, then the odd grids' last step.
+        if (step & 1) continue;
+        const int j = step / 2;
+        if (j < (int)c.active.size() && c.active[j] > 0) {
+          B_TRY(launch_class_step(c, c.active[j], j & 1, s),
+                "batch step launch");
+          ++n;
+        }
+        if (c.one_n[j] > 0) {
+          B_TRY(d3d::launch_pitched_strip(1, c.d_descs1,
+                                          c.d_items1 + c.one_lo[j],
+                                          c.one_n[j], j & 1, s,
+                                          d3d::device_error_word()),
+                "batch step launch");
+          ++n;
+        }
+        continue;
+      }
+      if (c.active[step] == 0) continue;
       B_TRY(launch_class_step(c, c.active[step], step & 1, s),
             "batch step launch");
       ++n;
@@ -404,7 +502,7 @@ int d3d_batch_create(const d3d_batch_grid* grids, int n, void* arena,
       d3d_batch_destroy(b);
       return rc;
     }
-    for (int st = 0; st < c.max_steps; ++st) b->total_items += c.active[st];
+    for (int a : c.active) b->total_items += a;
   }
   int rc = build_repitch(b);
   if (rc) {
@@ -428,11 +526,12 @@ int d3d_batch_autotune(d3d_batch b, void* stream) {
   for (int ci = 0; ci < kNumClasses; ++ci) {
     ClassPlan& c = b->cls[ci];
     if (c.grids.empty()) continue;
-    const int probe_steps = std::min(c.max_steps, 8);
+    const int probe_steps = std::min(c.max_steps, 8);  // pairs count 2
     if (probe_steps == 0) continue;
     float best = -1.0f;
     int best_kind = c.kind;
     for (int kind = 0; kind < kNumKinds; ++kind) {
+      if (kind_two(kind) && !class_takes_two_step(b, c)) continue;
       c.kind = kind;
       int rc = build_class(b, c);
       if (rc) return rc;
@@ -455,7 +554,7 @@ int d3d_batch_autotune(d3d_batch b, void* stream) {
     if (rc) return rc;
   }
   for (const ClassPlan& c : b->cls)
-    for (int st = 0; st < c.max_steps; ++st) b->total_items += c.active[st];
+    for (int a : c.active) b->total_items += a;
   return build_repitch(b);
 }
 
@@ -463,13 +562,18 @@ int d3d_batch_set_kind(d3d_batch b, int kind) {
   if (!b) return bfail(D3D_E_INVALID, "NULL batch");
   if (kind < 0 || kind >= kNumKinds)
     return bfail(D3D_E_INVALID, "no such kernel kind");
+  if (kind_two(kind))
+    for (const ClassPlan& c : b->cls)
+      if (!class_takes_two_step(b, c))
+        return bfail(D3D_E_UNSUPPORTED,
+                     "two-step kinds need grids at most 248 floats wide");
   drop_graph(b);
   b->total_items = 0;
   for (ClassPlan& c : b->cls) {
     c.kind = kind;
     int rc = build_class(b, c);
     if (rc) return rc;
-    for (int st = 0; st < c.max_steps; ++st) b->total_items += c.active[st];
+    for (int a : c.active) b->total_items += a;
   }
   return build_repitch(b);
 }
@@ -539,9 +643,10 @@ int d3d_batch_info(d3d_batch b, char* buf, size_t len) {
     const int nr = kind_nr(c.kind);
     if (nr)
       used += snprintf(buf + used, len - used,
-                       "%s{\"grids\": %zu, \"kernel\": \"strip\", "
+                       "%s{\"grids\": %zu, \"kernel\": \"%s\", "
                        "\"segments_per_thread\": %d, \"items\": %d}",
-                       ci ? ", " : "", c.grids.size(), nr, c.nitems);
+                       ci ? ", " : "", c.grids.size(),
+                       kind_two(c.kind) ? "strip2" : "strip", nr, c.nitems);
     else
       used += snprintf(buf + used, len - used,
                        "%s{\"grids\": %zu, \"kernel\": \"march\", "
@@ -556,10 +661,7 @@ int d3d_batch_info(d3d_batch b, char* buf, size_t len) {
 int d3d_batch_destroy(d3d_batch b) {
   if (!b) return D3D_OK;
   drop_graph(b);
-  for (auto& c : b->cls) {
-    if (c.d_descs) cudaFree(c.d_descs);
-    if (c.d_items) cudaFree(c.d_items);
-  }
+  for (auto& c : b->cls) free_class(c);
   if (b->d_rep_in) cudaFree(b->d_rep_in);
   if (b->d_rep_out) cudaFree(b->d_rep_out);
   if (b->pitched) cudaFree(b->pitched);

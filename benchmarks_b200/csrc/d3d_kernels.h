@@ -173,6 +173,19 @@ cudaError_t launch_pitched_strip(int nr, const PitchedDesc* descs,
                                  const int2* items, int nitems, int parity,
                                  cudaStream_t s, unsigned* dev_err);
 
+// Two fused steps per pass, strip form (NR = 1 or 2 level-2 segments a
+// thread), for grids whose pitch is one piece (px <= kStripMaxW; pieces = 0
+// from strip2_shape otherwise).  Items: tiles_x = 1, tiles_xy = strips,
+// zc = z slab.  Tensor-map box: (px + 8) x (rows + 4), from y0 - 2.  A
+// pass reads map[parity] and writes the other buffer two steps later.
+__host__ __device__ constexpr int strip2_slot_bytes(int nr) {
+  return nr * 6656;
+}
+StripShape strip2_shape(int px, int ny, int nr);
+cudaError_t launch_pitched_strip2(int nr, const PitchedDesc* descs,
+                                  const int2* items, int nitems, int parity,
+                                  cudaStream_t s, unsigned* dev_err);
+
 // One grid of a multi-grid repitch: `rows` (= ny * nz) rows of nx floats
 // at `dense`, px floats at `pitched`.
 struct RepitchDesc {

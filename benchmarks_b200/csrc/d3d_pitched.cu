@@ -427,6 +427,218 @@ drain:
   __syncthreads();
 }
 
+// ---------------------------------------------------------------------------
+// Two fused steps per pass, strip form.  For grids whose pitch fits one
+// piece (px <= kStripMaxW) a strip spans whole rows, so the intermediate
+// level needs a y halo (one row above and below) and a z halo, and no x
+// halo at all.  Level 0 is TMA-loaded as (4 * segs + 8) x (rows + 4)
+// boxes into a 4-stage ring; level 1 is computed over rows + 2 rows into a
+// 4-slot shared ring; level 2 reads its b, c, t, n, s from that ring and
+// stores to HBM.  Both levels map threads linearly onto their own (row,
+// segment) pairs, so neither wastes lanes.  In iteration q level 1 makes
+// plane q-1 and level 2 plane q-3, which reads only ring planes written in
+// earlier iterations: one block barrier per plane.  Every operand is a
+// shared-memory load (no register queues, since the two levels' thread
+// maps differ by a row), so a fused pair issues more instructions than two
+// single strip steps; on B200 the batch autotuner measures it (temporal-
+// block depth 2) against the single-step kinds per size class.
+// ---------------------------------------------------------------------------
+template <int NR>
+__global__ void __launch_bounds__(256, 4 / NR)
+    pitched_strip2_kernel(const PitchedDesc* __restrict__ descs,
+                          const int2* __restrict__ items, int parity,
+                          unsigned* __restrict__ dev_err) {
+  constexpr int S0 = 4, V = 4, HX = 4, NR1 = NR + 1;
+  constexpr int STAGE = strip2_slot_bytes(NR);  // level-0 stage
+  constexpr int SLOT = strip2_slot_bytes(NR);   // level-1 ring slot
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  float* stages = reinterpret_cast<float*>(base);
+  float* ring = reinterpret_cast<float*>(base + S0 * STAGE);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + S0 * STAGE + 4 * SLOT);
+
+  const int2 it = items[blockIdx.x];
+  const PitchedDesc* dp = descs + it.x;
+  const CUtensorMap* src = &dp->map[parity];
+  float* __restrict__ dst = parity ? dp->a : dp->b;
+  const int nx = dp->nx, px = dp->px, ny = dp->ny, nz = dp->nz;
+  const int segs = dp->seg_w, rows = dp->rows;
+  const int pw = V * segs + 2 * HX;  // row pitch of stages and ring
+  const unsigned box_bytes = (unsigned)(pw * (rows + 4)) * 4u;
+  const int y0 = (it.y % dp->tiles_xy) * rows;
+  const int z0 = (it.y / dp->tiles_xy) * dp->zc;
+  const int z1 = min(nz, z0 + dp->zc);
+  if (z0 >= z1) return;
+  const Coef<float> k{dp->k[0], dp->k[1], dp->k[2], dp->k[3],
+                      dp->k[4], dp->k[5], dp->k[6], dp->k[7]};
+  // Level-1 planes [lo1, hi1], level-0 planes [lo0, hi0].
+  const int lo1 = max(z0 - 1, 0), hi1 = min(z1, nz - 1);
+  const int lo0 = max(z0 - 2, 0), hi0 = min(z1 + 1, nz - 1);
+
+  auto stage_of = [&](int p) { return (int)((unsigned)(p - lo0) % S0); };
+  auto parity_of = [&](int p) { return ((unsigned)(p - lo0) / S0) & 1u; };
+  auto stage_ptr = [&](int p) { return stages + stage_of(p) * (STAGE / 4); };
+  auto ring_ptr = [&](int p) { return ring + (p & 3) * (SLOT / 4); };
+  auto issue = [&](int p) {
+    const int s = stage_of(p);
+    mbar_arrive_expect_tx(&bars[s], box_bytes);
+    tma_load_3d(stages + s * (STAGE / 4), src, &bars[s], -HX, y0 - 2, p);
+  };
+
+  if (threadIdx.x == 0) {
+    tensormap_acquire(src);
+    tma_prefetch_desc(src);
+    for (int s = 0; s < S0; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  int issued_hi = min(hi0, lo0 + S0 - 1);  // same value in every thread
+  if (threadIdx.x == 0)
+    for (int p = lo0; p <= issued_hi; ++p) issue(p);
+
+  // Addressing shared by both levels for a (row r of the ring / stage
+  // frame, segment): offset r * pw + HX + 4 * seg.  Level-1 row r1 is
+  // y = y0 - 1 + r1 (stage row r1 + 1, ring row r1); level-2 row r2 is
+  // y = y0 + r2 (ring row r2 + 1).  Rules: y = 0 / ny-1 read the centre
+  // row as n / s; x = 0 takes the centre value as w; x = nx-1 in a full
+  // last segment takes the centre value as e, a padded one reads its pad;
+  // a row's or warp's edge segment reads the word beside it.
+  const int lane = threadIdx.x & 31;
+  struct Cell {
+    int c, n, s;     // offsets within a stage or ring plane
+    bool w_sm, w_own, e_sm, e_own, cross, live;
+    int jh;
+  };
+  auto make_cell = [&](int L, int nrows, int frame_row0, int yoff,
+                       size_t* g_off) {
+    Cell cl;
+    int row = L / segs;
+    const int seg = L - row * segs;
+    cl.live = row < nrows;
+    row = min(row, nrows - 1);
+    const int y = yoff + row, xg = V * seg;
+    cl.c = (frame_row0 + row) * pw + HX + V * seg;
+    cl.n = (y == 0) ? cl.c : cl.c - pw;
+    cl.s = (y >= ny - 1) ? cl.c : cl.c + pw;
+    cl.w_own = (xg == 0);
+    cl.w_sm = !cl.w_own && (seg == 0 || lane == 0);
+    cl.e_own = (xg + V - 1 == nx - 1);
+    cl.e_sm = !cl.e_own && (seg == segs - 1 || lane == 31);
+    cl.cross = (xg < nx) && (xg + V > nx);
+    cl.jh = nx - 1 - xg;
+    if (g_off) {
+      *g_off = (size_t)y * px + xg;
+      cl.live = cl.live && y < ny && xg < px;
+    }
+    return cl;
+  };
+  Cell c1[NR1], c2[NR];
+  size_t g_off[NR];
+#pragma unroll
+  for (int j = 0; j < NR1; ++j)
+    c1[j] = make_cell(j * 256 + (int)threadIdx.x, rows + 2, 1, y0 - 1,
+                      nullptr);
+#pragma unroll
+  for (int r = 0; r < NR; ++r)
+    c2[r] = make_cell(r * 256 + (int)threadIdx.x, rows, 1, y0, &g_off[r]);
+  const size_t plane = (size_t)px * ny;
+  const Coef2 kk = coef2(k);
+
+  // One segment from a plane frame: c, n, s, w, e from plane `pc`, b and t
+  // from planes `pb`, `pt` (same offsets).
+  auto seg_point = [&](const Cell& cl, const float* pc, const float* pb,
+                       const float* pt) {
+    const V16<float> c = ld16_shared(pc + cl.c);
+    const V16<float> n = ld16_shared(pc + cl.n);
+    const V16<float> s = ld16_shared(pc + cl.s);
+    const V16<float> b = ld16_shared(pb + cl.c);
+    const V16<float> t = ld16_shared(pt + cl.c);
+    float wl = __shfl_up_sync(0xffffffffu, c.e[V - 1], 1);
+    float er = __shfl_down_sync(0xffffffffu, c.e[0], 1);
+    wl = ld_shared_if(cl.w_sm, pc + cl.c - 1, wl);
+    if (cl.w_own) wl = c.e[0];
+    er = ld_shared_if(cl.e_sm, pc + cl.c + V, er);
+    if (cl.e_own) er = c.e[V - 1];
+    V16<float> o = point_seg<float>(kk, c, n, s, b, t, wl, er);
+    if (cl.cross) {
+      if (cl.jh < 1) o.e[1] = o.e[0];
+      if (cl.jh < 2) o.e[2] = o.e[1];
+      o.e[3] = o.e[2];
+    }
+    return o;
+  };
+
+  const int qs = lo1 + 1, qe = z1 + 2;
+  int qf = -1;  // the iteration whose wait ran out
+  {
+    bool ok = true;
+    for (int p = lo0; p <= min(qs, hi0); ++p)
+      ok = ok && mbar_wait_bounded(&bars[stage_of(p)], parity_of(p));
+    if (!__syncthreads_and(ok)) {
+      if (threadIdx.x == 0) atomicOr(dev_err, kDevWaitTimeout);
+      qf = lo0 - 1;
+    }
+  }
+  if (qf < 0) {
+    for (int q = qs; q <= qe; ++q) {
+      const int p1 = q - 1, p2 = q - 3;
+      if (p1 <= hi1) {  // level 1: plane p1 into the ring
+        const float* pc = stage_ptr(p1);
+        const float* pb = stage_ptr(max(p1 - 1, 0));
+        const float* pt = stage_ptr(min(p1 + 1, nz - 1));
+        float* out = ring_ptr(p1);
+#pragma unroll
+        for (int j = 0; j < NR1; ++j) {
+          const V16<float> o = seg_point(c1[j], pc, pb, pt);
+          if (c1[j].live)
+            *reinterpret_cast<V16<float>*>(out + c1[j].c - pw) = o;
+        }
+      }
+      if (p2 >= z0) {  // level 2: plane p2 to HBM
+        const float* pc = ring_ptr(p2);
+        const float* pb = ring_ptr(max(p2 - 1, 0));
+        const float* pt = ring_ptr(min(p2 + 1, nz - 1));
+        float* out = dst + (size_t)p2 * plane;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          const V16<float> o = seg_point(c2[r], pc, pb, pt);
+          if (c2[r].live) st16_global(out + g_off[r], o);
+        }
+      }
+      // Level 1 of the next iteration needs level-0 plane q+1.
+      bool ok2 = true;
+      if (q + 1 <= hi0)
+        ok2 = mbar_wait_bounded(&bars[stage_of(q + 1)], parity_of(q + 1));
+      if (!__syncthreads_and(ok2)) {
+        if (threadIdx.x == 0) atomicOr(dev_err, kDevWaitTimeout);
+        qf = q;
+        break;
+      }
+      // Plane q-2 is free now (its last reader was this level-1 plane).
+      if (q - 2 >= lo0 && q - 2 + S0 <= hi0) {
+        if (threadIdx.x == 0) issue(q - 2 + S0);
+        issued_hi = q - 2 + S0;
+      }
+    }
+  }
+  if (qf < 0) return;
+  // A wait ran out: let every load issued and not yet waited for land
+  // (bounded) before the CTA exits.
+  if (threadIdx.x == 0) {
+    for (int p = max(qf + 1, lo0); p <= issued_hi; ++p) {
+      bool done = false;
+      for (unsigned i = 0; i < (kMaxWaitIters >> 4) && !done; ++i)
+        done = mbar_try_wait(&bars[stage_of(p)], parity_of(p));
+      if (!done) {
+        atomicOr(dev_err, kDevDrainTimeout);
+        break;
+      }
+    }
+  }
+  __syncthreads();
+}
+
 // Between the host's dense rows (nx floats) and the arena's pitched rows
 // (px floats): `to_pitched` writes every x in [0, px) of dst from
 // src[min(x, nx-1)], which also fills the pads; otherwise dst takes the
@@ -556,6 +768,42 @@ cudaError_t launch_pitched_strip(int nr, const PitchedDesc* descs,
   if (nr == 2)
     return go(pitched_strip_kernel<2, 3>,
               4 * strip_stage_bytes(2) + 4 * 8 + 128);
+  return cudaErrorInvalidValue;
+}
+
+StripShape strip2_shape(int px, int ny, int nr) {
+  StripShape sh{1, px / 4, 1};
+  if (px > kStripMaxW) {  // no two-step form: the strip needs x halos
+    sh.pieces = 0;
+    return sh;
+  }
+  const int pw = px + 8;
+  sh.rows = std::max(1, std::min({64, ny, nr * 256 / sh.segs}));
+  while (sh.rows > 1 && pw * (sh.rows + 4) * 4 > strip2_slot_bytes(nr))
+    --sh.rows;
+  return sh;
+}
+
+cudaError_t launch_pitched_strip2(int nr, const PitchedDesc* descs,
+                                  const int2* items, int nitems, int parity,
+                                  cudaStream_t s, unsigned* dev_err) {
+  if (nitems <= 0) return cudaSuccess;
+  auto go = [&](auto kern, int smem) {
+    static bool attr_set[2] = {false, false};
+    bool& set = attr_set[nr - 1];
+    if (!set) {
+      cudaError_t e = cudaFuncSetAttribute(
+          kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e != cudaSuccess) return e;
+      set = true;
+    }
+    kern<<<nitems, 256, smem, s>>>(descs, items, parity, dev_err);
+    return cudaGetLastError();
+  };
+  if (nr == 1)
+    return go(pitched_strip2_kernel<1>, 8 * strip2_slot_bytes(1) + 4 * 8 + 128);
+  if (nr == 2)
+    return go(pitched_strip2_kernel<2>, 8 * strip2_slot_bytes(2) + 4 * 8 + 128);
   return cudaErrorInvalidValue;
 }
 

@@ -250,15 +250,18 @@ int d3d_batch_layout(d3d_batch_grid* grids, int n, size_t* arena_bytes);
 int d3d_batch_create(const d3d_batch_grid* grids, int n, void* arena,
                      size_t arena_bytes, d3d_batch* out);
 
-/* Times each kernel kind (4 march tile shapes, 2 strip forms) per size
- * class on the batch's own grids (their fields are overwritten) and keeps
- * the fastest per class. */
+/* Times each kernel kind (4 march tile shapes, 2 strip forms, and 2
+ * two-step strip forms where the class's grids allow) per size class on
+ * the batch's own grids (their fields are overwritten) and keeps the
+ * fastest per class: tile shape and temporal-block depth per class. */
 int d3d_batch_autotune(d3d_batch batch, void* stream);
 
 /* Sets every size class to one kernel kind: 0..3 the march kernel with
  * tile 32x16 (x pairs), 64x8 (x pairs), 32x8, 16x16; 4 and 5 the strip
  * kernel with 1 or 2 segments a thread (4 is the default before
- * d3d_batch_autotune). */
+ * d3d_batch_autotune); 6 and 7 its two-step form (temporal-block depth 2:
+ * fused step pairs, and one strip step to finish an odd step count),
+ * D3D_E_UNSUPPORTED if a grid is wider than 248 floats. */
 int d3d_batch_set_kind(d3d_batch batch, int kind);
 
 /* Runs every grid for its step count: the first call captures the run

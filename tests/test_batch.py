@@ -148,16 +148,17 @@ def test_autotuned_batch_still_bit_exact():
         if c["kernel"] == "march":
             assert tuple(c["tile"]) in {(64, 8), (32, 16), (32, 8), (16, 16)}
         else:
-            assert c["kernel"] == "strip"
+            assert c["kernel"] in ("strip", "strip2")
             assert c["segments_per_thread"] in (1, 2)
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kind", range(6))
+@pytest.mark.parametrize("kind", range(8))
 def test_every_kernel_kind_bit_exact(kind):
-    """Each march tile shape and both strip forms on grids of every size
-    class, nx leaving 0..3 pad columns in the pitched copies (nx = 1
-    included), zero-step grids, odd and even step counts."""
+    """Each march tile shape, both strip forms and both two-step strip
+    forms on grids of every size class, nx leaving 0..3 pad columns in the
+    pitched copies (nx = 1 included), zero-step grids, odd and even step
+    counts (a two-step class ends odd counts with one strip step)."""
     dims = [(1, 1, 1), (1, 5, 7), (3, 2, 9), (17, 23, 5), (24, 9, 13),
             (25, 30, 2), (40, 41, 11), (41, 3, 6), (72, 17, 8), (73, 70, 9),
             (96, 96, 4), (13, 1, 30)]
@@ -170,6 +171,19 @@ def test_every_kernel_kind_bit_exact(kind):
         assert o.tobytes() == O.run(f, c, steps).tobytes(), (kind, nx, ny,
                                                               nz, steps)
     assert B.check_device_errors() == 0
+
+
+@pytest.mark.gpu
+def test_two_step_kinds_need_narrow_grids():
+    specs = [(249, 3, 4, 2, B.batch_coefficients(249, 3, 4, 0.1)),
+             (20, 20, 20, 3, B.batch_coefficients(20, 20, 20, 0.1))]
+    batch = B.Batch(specs)
+    with pytest.raises(B.D3DError) as ei:
+        batch.set_kind(6)
+    assert ei.value.code == B.D3D_E_UNSUPPORTED
+    batch.set_kind(5)
+    batch.autotune()  # skips the two-step kinds for the wide grid's class
+    batch.close()
 
 
 @pytest.mark.gpu
