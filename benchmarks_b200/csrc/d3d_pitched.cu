@@ -310,8 +310,8 @@ __global__ void __launch_bounds__(256, MINB)
   // value, a padded one reads its pad (a copy of nx-1); a row's last
   // segment and lane 31 read the word after the segment.
   const int lane = threadIdx.x & 31;
-  int c_off[NR], n_off[NR], s_off[NR], jh[NR];
-  size_t g_off[NR];
+  // g_off: within one plane (px * ny < 2^31 points, checked at submit).
+  int c_off[NR], n_off[NR], s_off[NR], jh[NR], g_off[NR];
   bool store_ok[NR], w_sm[NR], w_own[NR], e_sm[NR], e_own[NR], cross[NR];
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(256, MINB)
     c_off[r] = (row + 1) * pw + HX + V * seg;
     n_off[r] = (yg == 0) ? c_off[r] : c_off[r] - pw;
     s_off[r] = (yg >= ny - 1) ? c_off[r] : c_off[r] + pw;
-    g_off[r] = (size_t)yg * px + xg;
+    g_off[r] = yg * px + xg;
     store_ok[r] = valid && yg < ny && xg < px;
     w_own[r] = (xg == 0);
     w_sm[r] = !w_own[r] && (seg == 0 || lane == 0);
