@@ -509,6 +509,11 @@ def run_b200(args):
             "zchunk": inf["launch_zchunk"], "smem": inf["smem"]}
         ptb.close()
 
+    # --- HBM calibration: out = cc * in over the same 512^3 buffers (the
+    # stencil's 8 B per point with no neighbours; d3d_copy_calibrate) ------
+    B.copy_calibrate(a, b, passes=2, stream=stream)  # warm-up
+    copy_ms, copy_gbs = B.copy_calibrate(a, b, passes=20, stream=stream)
+
     # --- correctness report: FP32 vs FP64 vs analytic, FP64 norms -------
     plan64 = B.Plan(n, n, n, B.F64, B.KERNEL_AUTO)
     c64 = plan64.reference_coefficients()
@@ -582,7 +587,12 @@ def run_b200(args):
                      "traffic": traffic,
                      "kernel": info["last_kernel"],
                      "updates_per_point_per_launch": updates_per_launch,
-                     "algorithmic_bytes_per_launch": algo_bytes},
+                     "algorithmic_bytes_per_launch": algo_bytes,
+                     "copy_calibration": {
+                         "gbs": copy_gbs, "frac_of_peak": copy_gbs / peak,
+                         "kernel_frac_of_copy": achieved / copy_gbs,
+                         "what": "20 ping-pong passes of f2 = cc*f1 over "
+                                 "two 512 MiB buffers (d3d_copy_calibrate)"}},
         "clocks": clocks,
         "e2e": e2e,
         "gpu_launches": launches,

@@ -73,6 +73,8 @@ _SIGNATURES = {
     "d3d_batch_layout": ([_vp, _i, ctypes.POINTER(ctypes.c_size_t)], _i),
     "d3d_batch_create": ([_vp, _i, _vp, _sz, _vpp], _i),
     "d3d_batch_autotune": ([_vp, _vp], _i),
+    "d3d_copy_calibrate": ([_vp, _vp, _sz, ctypes.c_float, _i, _vp,
+                            ctypes.POINTER(ctypes.c_float)], _i),
     "d3d_batch_set_kind": ([_vp, _i], _i),
     "d3d_batch_run": ([_vp, _vp, ctypes.POINTER(ctypes.c_float)], _i),
     "d3d_batch_info": ([_vp, ctypes.c_char_p, _sz], _i),
@@ -393,6 +395,19 @@ class BatchGrid(ctypes.Structure):
                 ("coeff", ctypes.c_float * 7),
                 ("offset_a", ctypes.c_ulonglong),
                 ("offset_b", ctypes.c_ulonglong)]
+
+
+def copy_calibrate(f1, f2, passes=10, cc=0.4, stream=None):
+    """HBM calibration (d3d_copy_calibrate): `passes` ping-pong passes of
+    f2 = cc * f1 over two float32 CUDA tensors of equal size; returns
+    (device ms, GB/s at 8 bytes per point per pass)."""
+    assert str(f1.dtype) == "torch.float32" == str(f2.dtype)
+    assert f1.numel() == f2.numel()
+    ms = ctypes.c_float()
+    check(lib().d3d_copy_calibrate(f1.data_ptr(), f2.data_ptr(), f1.numel(),
+                                   cc, passes, _stream_handle(stream),
+                                   ctypes.byref(ms)))
+    return ms.value, 8.0 * f1.numel() * passes / (ms.value * 1e-3) / 1e9
 
 
 def batch_coefficients(nx, ny, nz, kappa):

@@ -753,6 +753,38 @@ int d3d_analytic(d3d_plan p, void* out, double time, void* stream) {
   return D3D_OK;
 }
 
+int d3d_copy_calibrate(const float* f1, float* f2, size_t n, float cc,
+                       int passes, void* stream, float* ms) {
+  if (!f1 || !f2 || passes < 1) return fail(D3D_E_INVALID, "bad arguments");
+  const uintptr_t a = reinterpret_cast<uintptr_t>(f1);
+  const uintptr_t b = reinterpret_cast<uintptr_t>(f2);
+  if (a < b + n * sizeof(float) && b < a + n * sizeof(float))
+    return fail(D3D_E_INVALID, "the two buffers overlap");
+  cudaStream_t s = as_stream(stream);
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  cudaError_t e = cudaEventCreate(&ev[0]);
+  if (e == cudaSuccess) e = cudaEventCreate(&ev[1]);
+  if (e == cudaSuccess) e = cudaEventRecord(ev[0], s);
+  const float* in = f1;
+  float* out = f2;
+  for (int i = 0; i < passes && e == cudaSuccess; ++i) {
+    e = d3d::launch_scale_copy(in, out, n, cc, s);
+    const float* t = in;
+    in = out;
+    out = const_cast<float*>(t);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(ev[1], s);
+  if (e == cudaSuccess) e = cudaEventSynchronize(ev[1]);
+  float t_ms = 0.0f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t_ms, ev[0], ev[1]);
+  if (ev[0]) cudaEventDestroy(ev[0]);
+  if (ev[1]) cudaEventDestroy(ev[1]);
+  if (e != cudaSuccess) return cuda_fail(e, "copy calibration");
+  g_launches.fetch_add((unsigned long long)passes, std::memory_order_relaxed);
+  if (ms) *ms = t_ms;
+  return D3D_OK;
+}
+
 int d3d_compare(d3d_plan p, const void* a, int a_dtype, const void* b,
                 int b_dtype, size_t n, double out[4], void* stream) {
   if (!p || !a || !b || !out) return fail(D3D_E_INVALID, "NULL argument");

@@ -49,6 +49,11 @@ cudaError_t encode_field_map(CUtensorMap* map, const void* ptr, int nx, int ny,
 // 5th (diffusion3d, diffusion3d_openmp.cc:57-62); 1 sums y-1 4th and y+1
 // 5th (the diffusion::Diffusion surface, diffusion_openmp.cc:98-103).
 
+// out = cc * in over n floats (HBM calibration at the stencil's 8 bytes
+// per point).
+cudaError_t launch_scale_copy(const float* in, float* out, size_t n, float cc,
+                              cudaStream_t s);
+
 // One time step, f2 = stencil(f1), with the TMA-staged z-march.
 cudaError_t launch_step_tma(const CUtensorMap& src, void* f2, int nx, int ny,
                             int nz, const void* coef, int dtype, int variant,

@@ -449,4 +449,43 @@ cudaError_t launch_step_generic(const void* f1, void* f2, int nx, int ny,
 }
 
 
+// ---------------------------------------------------------------------------
+// HBM calibration: out = cc * in, the stencil's own traffic (4 bytes read,
+// 4 written per point) with no neighbours -- the measured ceiling the step
+// kernels are compared against.  The reference's DiffusionCUDACopy
+// (diffusion/diffusion_cuda_copy.cu:8-24) plays this role there.  16-byte
+// loads and stores in a grid-stride loop when both pointers are 16-byte
+// aligned, a scalar tail after them (or scalar throughout otherwise).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+    scale_copy_kernel(const float* __restrict__ in, float* __restrict__ out,
+                      size_t n, float cc, bool vec) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  size_t done = 0;
+  if (vec) {
+    const size_t nq = n / 4;
+    const float4* qi = reinterpret_cast<const float4*>(in);
+    float4* qo = reinterpret_cast<float4*>(out);
+    for (size_t q = i; q < nq; q += stride) {
+      const float4 v = qi[q];
+      qo[q] = make_float4(__fmul_rn(cc, v.x), __fmul_rn(cc, v.y),
+                          __fmul_rn(cc, v.z), __fmul_rn(cc, v.w));
+    }
+    done = nq * 4;
+  }
+  for (size_t j = done + i; j < n; j += stride) out[j] = __fmul_rn(cc, in[j]);
+}
+
+cudaError_t launch_scale_copy(const float* in, float* out, size_t n, float cc,
+                              cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const bool vec = ((reinterpret_cast<uintptr_t>(in) |
+                     reinterpret_cast<uintptr_t>(out)) & 15) == 0;
+  // Eight 256-thread CTAs per SM, each thread a few 16-byte loads in flight.
+  const int blocks = num_sms() * 8;
+  scale_copy_kernel<<<blocks, 256, 0, s>>>(in, out, n, cc, vec);
+  return cudaGetLastError();
+}
+
 }  // namespace d3d

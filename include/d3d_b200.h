@@ -205,6 +205,17 @@ int d3d_checkpoint_save_host(d3d_plan plan, const void* host_field,
 int d3d_compare(d3d_plan plan, const void* a, int a_dtype, const void* b,
                 int b_dtype, size_t n, double out[4], void* stream);
 
+/* HBM calibration: `passes` ping-pong passes of f2 = cc * f1 over n floats
+ * (then f1 = cc * f2, ...), 16-byte vectorised when both buffers are
+ * 16-byte aligned.  It moves the stencil's 8 bytes per point with no
+ * neighbours, so 8 * n * passes / time is the ceiling the step kernels
+ * are held to.  The counterpart of the reference's DiffusionCUDACopy
+ * (diffusion/diffusion_cuda_copy.cu:8-24).  *ms receives the device time
+ * (CUDA events on `stream`); synchronises `stream`.  The buffers must not
+ * overlap. */
+int d3d_copy_calibrate(const float* f1, float* f2, size_t n, float cc,
+                       int passes, void* stream, float* ms);
+
 /* ---------------------------------------------------------------------
  * Batched solves: many independent FP32 grids of different shapes,
  * coefficients and step counts advanced together -- one multi-grid step

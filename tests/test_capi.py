@@ -89,3 +89,38 @@ def test_diffusion_plan_rejects_bad_arguments():
             == B.D3D_E_UNSUPPORTED
     assert L.d3d_diffusion_coefficients(1, d2, B.F32, None, None) \
         == B.D3D_E_INVALID
+
+
+def test_copy_calibrate_rejects_bad_arguments():
+    """Argument checks run before any device work."""
+    L = B.lib()
+    ms = ctypes.c_float()
+    assert L.d3d_copy_calibrate(None, None, 8, 0.4, 1, None,
+                                ctypes.byref(ms)) == B.D3D_E_INVALID
+    # overlapping buffers
+    assert L.d3d_copy_calibrate(4096, 4096 + 16, 64, 0.4, 1, None,
+                                ctypes.byref(ms)) == B.D3D_E_INVALID
+    assert L.d3d_copy_calibrate(4096, 1 << 20, 64, 0.4, 0, None,
+                                ctypes.byref(ms)) == B.D3D_E_INVALID
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,offset", [(1 << 20, 0), (1000003, 0), (4099, 1),
+                                      (3, 0), (1, 2)])
+def test_copy_calibrate_scales_exactly(n, offset):
+    """One pass writes cc * f1 into f2 bit-exactly (16-byte vector body and
+    scalar tail, or scalar throughout for misaligned buffers); a second
+    pass writes cc * f2 back into f1."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(7)
+    buf1 = torch.rand(n + offset, device="cuda", generator=g)
+    buf2 = torch.zeros(n + offset, device="cuda")
+    f1, f2 = buf1[offset:], buf2[offset:]
+    x = f1.cpu().numpy().copy()
+    cc = np.float32(0.4)
+    ms, gbs = B.copy_calibrate(f1, f2, passes=1, cc=float(cc))
+    assert ms > 0 and gbs > 0
+    assert f2.cpu().numpy().tobytes() == (cc * x).astype(np.float32).tobytes()
+    B.copy_calibrate(f1, f2, passes=2, cc=float(cc))
+    y = (cc * (cc * x).astype(np.float32)).astype(np.float32)
+    assert f1.cpu().numpy().tobytes() == y.tobytes()
