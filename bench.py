@@ -161,16 +161,21 @@ def cpu_reference_leg(n_side, steps_hint=None, budget_s=12.0):
                           else "oracle port", t)}
 
 
-def batched_leg(B, torch, n_grids=4096, plain_sample=64):
+def batched_leg(B, torch, n_grids=4096, plain_sample=64, kind=None):
     """Config: 4096 grids, sides U{16..96} per axis, kappa U[0.05,0.2],
     steps U{10..500}; one batched run (one CUDA graph) vs a plain per-solve
     loop (a plan, two device buffers and a RunKernel-style d3d_run per
-    grid) on the first `plain_sample` grids."""
+    grid) on the first `plain_sample` grids.  `kind` forces one kernel kind
+    for every size class instead of the autotuner (for profiling: an
+    autotuner timed under a profiler picks differently)."""
     from benchmarks_b200.workloads import batched_specs
     specs = batched_specs(n_grids)
     updates = sum(nx * ny * nz * s for nx, ny, nz, s, _ in specs)
     batch = B.Batch(specs)
-    batch.autotune()
+    if kind is None:
+        batch.autotune()
+    else:
+        batch.set_kind(kind)
     batch.arena.uniform_(0.0, 1.0)
     batch.run()  # capture + first replay
     runs = [batch.run() for _ in range(3)]
@@ -630,22 +635,25 @@ def main():
                                            "diffusion2d"],
                     help="run one side leg alone on GPU 0 and print its "
                          "JSON (no headline line; for profiling)")
+    ap.add_argument("--batch-kind", type=int, default=None,
+                    help="with --only-leg batched: one kernel kind for "
+                         "every size class instead of the autotuner")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.only_leg:
-        return run_one_leg(args.only_leg)
+        return run_one_leg(args.only_leg, args.batch_kind)
     return run_b200(args)
 
 
-def run_one_leg(leg):
+def run_one_leg(leg, batch_kind=None):
     import torch
     import benchmarks_b200 as B
     torch.cuda.set_device(0)
     if leg == "batched":
-        out = batched_leg(B, torch)
+        out = batched_leg(B, torch, kind=batch_kind)
     elif leg == "serving":
         out = serving_leg(B, torch)
     else:
