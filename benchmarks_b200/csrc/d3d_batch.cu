@@ -303,10 +303,16 @@ int build_class(d3d_batch b, ClassPlan& c) {
     for (int j = 0; j < nl; ++j) c.active[j] += tiles;
   }
   c.nitems = (int)items.size();
-  int rc = nr ? upload(pdescs, reinterpret_cast<PitchedDesc**>(&c.d_descs),
-                       "batch descriptors")
-              : upload(descs, reinterpret_cast<BatchDesc**>(&c.d_descs),
-                       "batch descriptors");
+  int rc;
+  if (nr) {
+    PitchedDesc* d = nullptr;
+    rc = upload(pdescs, &d, "batch descriptors");
+    c.d_descs = d;
+  } else {
+    BatchDesc* d = nullptr;
+    rc = upload(descs, &d, "batch descriptors");
+    c.d_descs = d;
+  }
   if (!rc) rc = upload(items, &c.d_items, "batch items");
   if (!rc) rc = upload(pdescs1, &c.d_descs1, "batch descriptors");
   if (!rc) rc = upload(items1, &c.d_items1, "batch items");
@@ -481,10 +487,11 @@ int d3d_batch_create(const d3d_batch_grid* grids, int n, void* arena,
     b->poff[i] = pe;
     pe += 2 * pitched_elems(grids[i]);
   }
+  // Without room for them the batch runs the march kinds only, on the
+  // caller's fields.
   if (cudaMalloc(&b->pitched, pe * sizeof(float)) != cudaSuccess) {
     cudaGetLastError();
-    d3d_batch_destroy(b);
-    return bfail(D3D_E_OOM, "pitched copies of the batch");
+    b->pitched = nullptr;
   }
   for (int i = 0; i < n; ++i) {
     ClassPlan& c = b->cls[class_of(grids[i].nx)];
@@ -496,7 +503,7 @@ int d3d_batch_create(const d3d_batch_grid* grids, int n, void* arena,
     std::stable_sort(c.grids.begin(), c.grids.end(), [&](int x, int y) {
       return b->grids[x].steps > b->grids[y].steps;
     });
-    c.kind = kDefaultKind;
+    c.kind = b->pitched ? kDefaultKind : 0;
     int rc = build_class(b, c);
     if (rc) {
       d3d_batch_destroy(b);
@@ -531,6 +538,7 @@ int d3d_batch_autotune(d3d_batch b, void* stream) {
     float best = -1.0f;
     int best_kind = c.kind;
     for (int kind = 0; kind < kNumKinds; ++kind) {
+      if (kind_nr(kind) && !b->pitched) continue;
       if (kind_two(kind) && !class_takes_two_step(b, c)) continue;
       c.kind = kind;
       int rc = build_class(b, c);
@@ -562,6 +570,9 @@ int d3d_batch_set_kind(d3d_batch b, int kind) {
   if (!b) return bfail(D3D_E_INVALID, "NULL batch");
   if (kind < 0 || kind >= kNumKinds)
     return bfail(D3D_E_INVALID, "no such kernel kind");
+  if (kind_nr(kind) && !b->pitched)
+    return bfail(D3D_E_UNSUPPORTED,
+                 "no device memory was left for the pitched copies");
   if (kind_two(kind))
     for (const ClassPlan& c : b->cls)
       if (!class_takes_two_step(b, c))

@@ -256,8 +256,10 @@ int d3d_batch_layout(d3d_batch_grid* grids, int n, size_t* arena_bytes);
 
 /* Builds the batch: size classes by nx, each class's grids ordered by step
  * count, their descriptors and work items, and device memory for pitched
- * copies of every grid (two buffers of ceil4(nx)*ny*nz floats each).
- * `arena` must stay valid for the batch's lifetime. */
+ * copies of every grid (two buffers of ceil4(nx)*ny*nz floats each; if
+ * that allocation fails the batch runs the march kinds only, on the
+ * caller's fields, and d3d_batch_set_kind refuses the others with
+ * D3D_E_UNSUPPORTED).  `arena` must stay valid for the batch's lifetime. */
 int d3d_batch_create(const d3d_batch_grid* grids, int n, void* arena,
                      size_t arena_bytes, d3d_batch* out);
 
