@@ -463,7 +463,7 @@ int d3d_batch_create(const d3d_batch_grid* grids, int n, void* arena,
     const d3d_batch_grid& g = grids[i];
     if (g.nx < 1 || g.ny < 1 || g.nz < 1 || g.steps < 0)
       return bfail(D3D_E_INVALID, "bad grid dimensions or steps");
-    if ((long long)g.nx * g.ny >= (1LL << 31))
+    if (((long long)g.nx + 3) / 4 * 4 * g.ny >= (1LL << 31))
       return bfail(D3D_E_INVALID, "grid plane too large");
     const unsigned long long pts = (unsigned long long)g.nx * g.ny * g.nz;
     if ((g.offset_a + pts) * 4 > arena_bytes ||

@@ -540,7 +540,7 @@ int d3d_server_submit(d3d_server s, int nx, int ny, int nz, int steps,
   if (!s || !coeff || !host_in || !host_out)
     return sfail(D3D_E_INVALID, "NULL argument");
   if (nx < 1 || ny < 1 || nz < 1 || steps < 0 ||
-      (long long)nx * ny >= (1LL << 31))
+      ((long long)nx + 3) / 4 * 4 * ny >= (1LL << 31))
     return sfail(D3D_E_INVALID, "bad grid dimensions or steps");
   const int px = s->kernel >= 0 ? (nx + 3) / 4 * 4 : nx;
   const unsigned long long pts = (unsigned long long)px * ny * nz;

@@ -73,6 +73,11 @@ def test_create_rejects_bad_batches():
     arr[0].nx = 0
     assert L.d3d_batch_create(arr, 1, 4096, 4096 * 4,
                               ctypes.byref(h)) == B.D3D_E_INVALID
+    # a plane under 2^31 points whose padded rows (ceil4(nx)) are not
+    arr[0].nx, arr[0].ny, arr[0].nz = 46341, 46340, 1
+    assert 46341 * 46340 < 2 ** 31 <= 46344 * 46340
+    assert L.d3d_batch_create(arr, 1, 4096, 1 << 62,
+                              ctypes.byref(h)) == B.D3D_E_INVALID
 
 
 def _mixed_specs(seed, n, max_side=40, max_steps=24):
