@@ -206,3 +206,35 @@ def test_batch_replay_is_repeatable():
         results.append([batch.result(i).cpu().numpy().tobytes()
                         for i in range(len(specs))])
     assert results[0] == results[1] == results[2]
+
+
+@pytest.mark.gpu
+def test_more_grids_than_one_launch_row():
+    """70,000 grids: the repitch launches stride over grids in steps of
+    65,535 (the grid-y limit) and the step launch has 70,000 CTAs."""
+    torch = pytest.importorskip("torch")
+    n = 70000
+    shapes = [(1, 1, 1), (5, 2, 3), (3, 4, 2)]
+    specs = []
+    for i in range(n):
+        nx, ny, nz = shapes[i % 3]
+        specs.append((nx, ny, nz, 1 + (i % 2),
+                      B.batch_coefficients(nx, ny, nz, 0.1)))
+    batch = B.Batch(specs)
+    batch.arena.zero_()
+    fields = {}
+    for j in range(6):  # shape x step parity
+        nx, ny, nz = shapes[j % 3]
+        fields[j] = O.seeded_noise((nz, ny, nx), 50 + j, amplitude=1.0)
+    for i in (0, 1, 2, 3, 4, 5, n - 6, n - 5, n - 4, n - 3, n - 2, n - 1,
+              65534, 65535, 65536):
+        batch.input(i).copy_(torch.from_numpy(fields[i % 6]))
+    batch.run()
+    torch.cuda.synchronize()
+    for i in (0, 1, 2, 3, 4, 5, n - 6, n - 5, n - 4, n - 3, n - 2, n - 1,
+              65534, 65535, 65536):
+        nx, ny, nz, steps, c = specs[i]
+        want = O.run(fields[i % 6], c, steps)
+        assert batch.result(i).cpu().numpy().tobytes() == want.tobytes(), i
+    assert B.check_device_errors() == 0
+    batch.close()
