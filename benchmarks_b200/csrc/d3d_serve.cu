@@ -13,10 +13,11 @@
 // Step kernel.  By default the strip form of the pitched TMA kernel
 // (d3d_pitched.cu): each solve is stored with rows padded to a 16-byte
 // pitch and read through two tensor maps encoded at admission, whose box
-// is the solve's strip (whole rows of up to 248 columns).  Host copies stay dense and contiguous
-// (one transfer each way); a device pass spreads an input into the pitched
-// layout (filling the pads) and packs a result back.  d3d_server_set_kernel(-1)
-// selects the unpadded march kernel of the batch API instead.
+// is the solve's strip (whole rows of up to 248 columns).  Host copies
+// stay dense and contiguous (one transfer each way); a device pass spreads
+// an input into the pitched layout (filling the pads) and packs a result
+// back.  d3d_server_set_kernel picks the tile form instead (0..4) or the
+// unpadded march kernel of the batch API (-1).
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -35,7 +36,9 @@ constexpr unsigned long long kAlign = 64;  // elements (256 bytes)
 constexpr int kStripBase = d3d::kNumPitchedVariants;
 constexpr int kDefaultKernel = kStripBase + 1;  // strip, 2 segments
 constexpr int kMaxKernel = kStripBase + 1;
-int strip_nr(int kernel) { return kernel >= kStripBase ? kernel - kStripBase + 1 : 0; }
+int strip_nr(int kernel) {
+  return kernel >= kStripBase ? kernel - kStripBase + 1 : 0;
+}
 constexpr int kMaxLanes = 4;               // compute streams
 constexpr int kDefaultLanes = 4;
 
