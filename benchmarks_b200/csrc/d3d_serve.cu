@@ -96,6 +96,7 @@ struct Request {
   int px;  // row pitch in floats (nx, or nx rounded up to 4 when pitched)
   d3d::StripShape strip{};  // strip kernels: pieces, segments, rows
   int zc = 0, tiles = 0;  // this tick: planes per z slab, work items
+  int n = 0;              // this tick: steps to run
   int lane = 0;           // compute stream that runs all its steps
   float coeff[7];
   const float* host_in;
@@ -195,10 +196,13 @@ size_t dense_bytes(const Request* r) {
 // Starts the device->host copy of a finished solve.  A pitched result is
 // first made dense in the solve's other buffer (one device pass), so the
 // copy to the host is one contiguous transfer.
-int start_retire(d3d_server s, Request* r) {
-  const float* src = s->arena + (r->cur_a ? r->off_a : r->off_b);
+// `in_a`: the result is in buffer a.  Called on the solve's lane right
+// after its last step launch, so its copy-out does not wait for the rest
+// of the lane's tick.
+int start_retire(d3d_server s, Request* r, bool in_a) {
+  const float* src = s->arena + (in_a ? r->off_a : r->off_b);
   if (r->px != r->nx) {
-    float* dense = s->arena + (r->cur_a ? r->off_b : r->off_a);
+    float* dense = s->arena + (in_a ? r->off_b : r->off_a);
     S_TRY(d3d::launch_repitch(src, dense, r->nx, r->px,
                               (long long)r->ny * r->nz, false,
                               s->lane[r->lane]),
@@ -287,7 +291,7 @@ int admit(d3d_server s) {
           "cudaStreamWaitEvent");
     it = s->queued.erase(it);
     if (r->steps == 0) {
-      int rc = start_retire(s, r);
+      int rc = start_retire(s, r, true);
       if (rc) return rc;
     } else {
       s->active.push_back(r);
@@ -303,6 +307,9 @@ int admit(d3d_server s) {
 // planes (each slab re-reads the plane above and below it).
 constexpr long kSlabTarget = 8 * 148;
 constexpr int kMaxSlab = 32, kMinSlab = 16;
+// Steps per tick: chunk * clamp(ceil(remaining / (chunk * kStepHorizon)),
+// 1, kMaxStepMult).
+constexpr int kStepHorizon = 8, kMaxStepMult = 4;
 int slab_planes(int nz, int cap) {
   const int ns = (nz + cap - 1) / cap;
   return (nz + ns - 1) / ns;  // balanced slabs of at most `cap` planes
@@ -383,17 +390,27 @@ int advance(d3d_server s) {
     }
     if ((long)nitems >= kSlabTarget || cap / 2 < kMinSlab) break;
   }
+  // Steps this tick: `chunk`, or a multiple of it for solves with many
+  // steps left, so they do not set the makespan by needing more ticks than
+  // anyone else; their extra launches hold few items and overlap other
+  // lanes' work.
+  const int chunk = s->chunk;
+  int nj = 0;  // launches this tick (the most steps any solve runs)
+  for (Request* r : act) {
+    const int rem = r->steps - r->done;
+    const int mult = std::min(kMaxStepMult,
+                              std::max(1, (rem + chunk * kStepHorizon - 1) /
+                                              (chunk * kStepHorizon)));
+    r->n = std::min(rem, chunk * mult);
+    nj = std::max(nj, r->n);
+  }
   // Each lane's solves are contiguous.  Within a lane, the solves still
-  // stepping at sub-step j must be a prefix: order by the steps this tick
+  // stepping at launch j must be a prefix: order by the steps this tick
   // runs, then by slab depth, longest first, so a launch starts its
   // longest CTAs first and its tail is short.
-  const int chunk = s->chunk;
-  std::sort(act.begin(), act.end(), [chunk](const Request* x,
-                                            const Request* y) {
+  std::sort(act.begin(), act.end(), [](const Request* x, const Request* y) {
     if (x->lane != y->lane) return x->lane < y->lane;
-    const int nx_ = std::min(chunk, x->steps - x->done);
-    const int ny_ = std::min(chunk, y->steps - y->done);
-    if (nx_ != ny_) return nx_ > ny_;
+    if (x->n != y->n) return x->n > y->n;
     return x->zc > y->zc;
   });
   const size_t desc_size =
@@ -402,7 +419,7 @@ int advance(d3d_server s) {
   if (rc) return rc;
   // Per lane: first descriptor, first item, items active at sub-step j.
   size_t desc0[kMaxLanes + 1] = {}, item0[kMaxLanes + 1] = {};
-  std::vector<int> active_at((size_t)kMaxLanes * s->chunk, 0);
+  std::vector<int> active_at((size_t)kMaxLanes * nj, 0);
   size_t k = 0;
   for (size_t i = 0; i < act.size(); ++i) {
     Request* r = act[i];
@@ -446,9 +463,8 @@ int advance(d3d_server s) {
       d.k[7] = -0.0f;
     }
     for (int t = 0; t < r->tiles; ++t) st.h_items[k++] = make_int2((int)i, t);
-    const int n = std::min(s->chunk, r->steps - r->done);
-    for (int j = 0; j < n; ++j)
-      active_at[(size_t)r->lane * s->chunk + j] += r->tiles;
+    for (int j = 0; j < r->n; ++j)
+      active_at[(size_t)r->lane * nj + j] += r->tiles;
   }
   // Each lane copies its own descriptors and items and launches its
   // sub-steps on its stream; lanes never wait for one another.
@@ -469,8 +485,11 @@ int advance(d3d_server s) {
       S_TRY(cudaEventCreate(&st.done[l]), "cudaEventCreate");
     }
     S_TRY(cudaEventRecord(st.start[l], ls), "cudaEventRecord");
-    const int* act_l = active_at.data() + (size_t)l * s->chunk;
-    for (int j = 0; j < s->chunk && act_l[j] > 0; ++j) {
+    const int* act_l = active_at.data() + (size_t)l * nj;
+    // This lane's solves in launch order of their last step (they are
+    // sorted by n, descending): retire each right after it.
+    size_t fin = desc0[l + 1];
+    for (int j = 0; j < nj && act_l[j] > 0; ++j) {
       auto* pd = static_cast<d3d::PitchedDesc*>(st.d_desc);
       S_TRY(nr ? d3d::launch_pitched_strip(nr, pd, st.d_items + item0[l],
                                            act_l[j], j & 1, ls,
@@ -484,6 +503,13 @@ int advance(d3d_server s) {
                       st.d_items + item0[l], act_l[j], j & 1, ls),
             "server step launch");
       ++n_launch;
+      while (fin > desc0[l] && act[fin - 1]->n == j + 1) {
+        Request* r = act[--fin];
+        if (r->done + r->n >= r->steps) {
+          rc = start_retire(s, r, r->cur_a != (bool)(r->n & 1));
+          if (rc) return rc;
+        }
+      }
     }
     S_TRY(cudaEventRecord(st.done[l], ls), "cudaEventRecord");
     st.used[l] = true;
@@ -493,18 +519,12 @@ int advance(d3d_server s) {
   st.in_flight = true;
   st.timed = true;
   ++s->tick_index;
-  // Book-keeping, then start the copies of the solves that finished.
+  // Book-keeping (finished solves are already retiring).
   std::vector<Request*> still;
   for (Request* r : act) {
-    const int n = std::min(s->chunk, r->steps - r->done);
-    r->done += n;
-    if (n & 1) r->cur_a = !r->cur_a;
-    if (r->done >= r->steps) {
-      rc = start_retire(s, r);
-      if (rc) return rc;
-    } else {
-      still.push_back(r);
-    }
+    r->done += r->n;
+    if (r->n & 1) r->cur_a = !r->cur_a;
+    if (r->done < r->steps) still.push_back(r);
   }
   act.swap(still);
   return D3D_OK;
