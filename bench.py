@@ -125,49 +125,47 @@ class ClockSampler:
                 "reasons": sorted(reasons)}
 
 
-def cpu_reference_leg(n_side, steps_hint=None, budget_s=12.0):
-    """Times the reference's own Diffusion3DOpenMP::RunKernel on the host
-    (oracle/_ref), else the oracle port, on a bounded sample of the 512^3
-    workload.  Returns a cpu_baseline dict."""
+def cpu_reference_leg(n_side, repeats=2):
+    """Times the reference's own Diffusion3DOpenMP::RunKernel(200) on the
+    host (oracle/_ref), else the oracle port, on this workload's input:
+    `repeats` whole RunKernel(200) calls on all host threads.  Returns a
+    cpu_baseline dict."""
     import oracle as O
+    from benchmarks_b200.workloads import field_noise
     threads = os.cpu_count() or 1
     kind = "reference" if O.ref_available() else "port"
     n = n_side
-
-    def timed(count):
-        if kind == "reference":
-            t0 = time.perf_counter()
-            O.ref_run(n, n, n, count)
-            # ref_run includes the reference's InitializeBenchmark
-            # (host Initialize over 512^3); time it separately and remove.
-            return time.perf_counter() - t0
-        c, _ = O.params(n, n, n)
-        f = O.initialize(n, n, n)
-        t0 = time.perf_counter()
-        O.run(f, c, count)
-        return time.perf_counter() - t0
-
     O.set_threads(threads)
-    t0 = timed(0)  # setup cost only (allocation + Initialize)
-    t2 = timed(2) - t0
-    per_step = max(t2 / 2, 1e-3)
-    steps = steps_hint or int(max(2, min(COUNT, budget_s / per_step)))
-    t = timed(steps) - t0
-    rate = n ** 3 * steps / t / 1e9
+    c, _ = O.params(n, n, n)
+    fin = O.initialize(n, n, n)
+    fin += field_noise(fin.shape)
+    t = 0.0
+    for _ in range(repeats):
+        if kind == "reference":
+            _, _, secs = O.ref_run(n, n, n, COUNT, field=fin, coeff=c,
+                                   want_time=True, want_field=False)
+        else:
+            t0 = time.perf_counter()
+            O.run(fin, c, COUNT)
+            secs = time.perf_counter() - t0
+        t += secs
+    rate = float(n) ** 3 * COUNT * repeats / t / 1e9
     return {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": "%d^3 FP32, %d steps of Diffusion3DOpenMP::RunKernel "
-                      "(%s), %.2f s, setup excluded" % (
-                          n, steps, "oracle/_ref" if kind == "reference"
-                          else "oracle port", t)}
+            "sample": "%d^3 FP32, %d x RunKernel(%d) of Diffusion3DOpenMP "
+                      "(%s) on this workload's input, %.2f s in all, setup "
+                      "excluded" % (n, repeats, COUNT,
+                                    "oracle/_ref" if kind == "reference"
+                                    else "oracle port", t)}
 
 
 def batched_leg(B, torch, n_grids=4096, plain_sample=64, kind=None):
     """Config: 4096 grids, sides U{16..96} per axis, kappa U[0.05,0.2],
     steps U{10..500}; one batched run (one CUDA graph) vs a plain per-solve
     loop (a plan, two device buffers and a RunKernel-style d3d_run per
-    grid) on the first `plain_sample` grids.  `kind` forces one kernel kind
-    for every size class instead of the autotuner (for profiling: an
-    autotuner timed under a profiler picks differently)."""
+    grid) on the first `plain_sample` grids, which also checks those grids'
+    batched results bit for bit against their runs alone.  `kind` forces
+    one kernel kind for every size class instead of the autotuner (for
+    profiling: an autotuner timed under a profiler picks differently)."""
     from benchmarks_b200.workloads import batched_specs
     specs = batched_specs(n_grids)
     updates = sum(nx * ny * nz * s for nx, ny, nz, s, _ in specs)
@@ -176,27 +174,38 @@ def batched_leg(B, torch, n_grids=4096, plain_sample=64, kind=None):
         batch.autotune()
     else:
         batch.set_kind(kind)
-    batch.arena.uniform_(0.0, 1.0)
+    gen = torch.Generator(device="cuda").manual_seed(0xB47C)
+    batch.arena.uniform_(0.0, 1.0, generator=gen)
     batch.run()  # capture + first replay
     runs = [batch.run() for _ in range(3)]
     ms = min(runs)
     info = batch.info()
+    # A fresh seeded input, one more run, and the sampled grids' results.
+    batch.arena.uniform_(0.0, 1.0, generator=gen)
+    sample = specs[:plain_sample]
+    inputs = [batch.input(i).clone() for i in range(len(sample))]
+    batch.run()
+    torch.cuda.synchronize()
+    results = [batch.result(i).clone() for i in range(len(sample))]
     batch.close()
     del batch
     torch.cuda.empty_cache()
-    sample = specs[:plain_sample]
     upd_s = sum(nx * ny * nz * s for nx, ny, nz, s, _ in sample)
     torch.cuda.synchronize()
+    alone = []
     t0 = time.perf_counter()
-    for (nx, ny, nz, s, c) in sample:
+    for (nx, ny, nz, s, c), fin in zip(sample, inputs):
         p = B.Plan(nx, ny, nz)
         p.set_graphs(False)
-        f1 = p.empty()
+        f1 = fin.clone()
         f2 = p.empty()
-        p.run(f1, f2, s, c)
+        res, _ = p.run(f1, f2, s, c)
         torch.cuda.synchronize()
+        alone.append(res)
         p.close()
     t_plain = time.perf_counter() - t0
+    mismatched = sum(1 for r, a in zip(results, alone)
+                     if not torch.equal(r, a))
     plain_solves = len(sample) / t_plain
     solves = n_grids / (ms / 1e3)
     return {"grids": n_grids, "updates": updates, "ms": ms,
@@ -204,26 +213,33 @@ def batched_leg(B, torch, n_grids=4096, plain_sample=64, kind=None):
             "unit": UNIT, "launches_per_run": info["launches_per_run"],
             "class_kernels": [
                 c["kernel"] + (" %dx%d" % tuple(c["tile"]) if "tile" in c
-                               else " x%d" % c["segments_per_thread"])
+                               else " x%d" % c["segments_per_thread"]
+                               if "segments_per_thread" in c else "")
                 for c in info["classes"]],
+            "info": info,
             "plain_loop": {"sample_grids": len(sample),
                            "solves_per_s": plain_solves,
                            "value": upd_s / t_plain / 1e9},
+            "results_equal_alone": {"grids_checked": len(sample),
+                                    "mismatched": mismatched},
             "speedup_solves": solves / plain_solves}
 
 
-def serving_leg(B, torch, n_req=96, arena_gb=24.0, chunk=8):
+def serving_leg(B, torch, n_req=256, arena_gb=24.0, chunk=8):
     """Config: Poisson stream (mean 2000 req/s) of cubic FP32 solves, sides
     log-uniform in [32, 256], steps log-uniform in [10, 2000]; the
     continuous-batching server vs a plain per-request loop (allocate,
     RunKernel with host copies, free) over the same arrivals.  Latency is
-    completion time minus scheduled arrival."""
+    completion time minus scheduled arrival.  Every served result is
+    compared bit for bit with the same request run alone (the plain loop)."""
     from benchmarks_b200.workloads import serving_requests
     reqs = serving_requests(n_req)
     sizes = [s ** 3 for _, s, _ in reqs]
     maxn = max(sizes)
-    pool_in = torch.rand(maxn, pin_memory=True).numpy()
-    out_pool = torch.empty(sum(sizes), pin_memory=True).numpy()
+    gen = torch.Generator().manual_seed(0x5E7F)
+    pool_in = torch.rand(maxn, generator=gen).pin_memory().numpy()
+    out_served = torch.empty(sum(sizes), pin_memory=True).numpy()
+    out_other = torch.empty(sum(sizes), pin_memory=True).numpy()
     offs = np.cumsum([0] + sizes[:-1])
     coeff = {}
     for _, s, _ in reqs:
@@ -239,7 +255,11 @@ def serving_leg(B, torch, n_req=96, arena_gb=24.0, chunk=8):
             np.percentile(lat, 99)), "makespan_s": span,
             "value": upd / span / 1e9}
 
-    def serve(kernel=None, lanes=None):
+    def out_view(pool, i):
+        s = reqs[i][1]
+        return pool[offs[i]:offs[i] + s ** 3].reshape(s, s, s)
+
+    def serve(out_pool, kernel=None, lanes=None):
         server = B.Server(int(arena_gb * 2 ** 30), chunk, kernel, lanes)
         done_at = [0.0] * n_req
         idmap = {}
@@ -250,8 +270,8 @@ def serving_leg(B, torch, n_req=96, arena_gb=24.0, chunk=8):
             while nxt < n_req and reqs[nxt][0] <= now:
                 _, s, st = reqs[nxt]
                 hin = pool_in[:s ** 3].reshape(s, s, s)
-                hout = out_pool[offs[nxt]:offs[nxt] + s ** 3].reshape(s, s, s)
-                idmap[server.submit(hin, hout, st, coeff[s])] = nxt
+                idmap[server.submit(hin, out_view(out_pool, nxt), st,
+                                    coeff[s])] = nxt
                 nxt += 1
             for rid in server.tick():
                 done_at[idmap[rid]] = time.perf_counter() - t0
@@ -262,11 +282,17 @@ def serving_leg(B, torch, n_req=96, arena_gb=24.0, chunk=8):
         server.close()
         return out
 
+    def same_results(a_pool, b_pool):
+        return sum(1 for i in range(n_req)
+                   if not np.array_equal(out_view(a_pool, i).view(np.uint32),
+                                         out_view(b_pool, i).view(np.uint32)))
+
     # served: the default server (pitched TMA step kernel, several
     # streams), then the same stream through the batch API's march kernel
     # on one stream for comparison
-    served = serve()
-    march = serve(kernel=-1, lanes=1)
+    served = serve(out_served)
+    march = serve(out_other, kernel=-1, lanes=1)
+    march_mismatched = same_results(out_served, out_other)
     # plain per-request loop
     import ctypes
     done_at = [0.0] * n_req
@@ -281,7 +307,7 @@ def serving_leg(B, torch, n_req=96, arena_gb=24.0, chunk=8):
         d1, d2 = ctypes.c_void_p(), ctypes.c_void_p()
         B.check(B.lib().d3d_device_alloc(n * 4, ctypes.byref(d1)))
         B.check(B.lib().d3d_device_alloc(n * 4, ctypes.byref(d2)))
-        host = out_pool[offs[i]:offs[i] + n]
+        host = out_other[offs[i]:offs[i] + n]
         host[:] = pool_in[:n]
         ms = ctypes.c_float()
         B.check(B.lib().d3d_run_host(p.handle, host.ctypes.data, d1, d2,
@@ -297,6 +323,11 @@ def serving_leg(B, torch, n_req=96, arena_gb=24.0, chunk=8):
             "served_march_one_stream": {
                 k: march[k] for k in ("solves_per_s", "makespan_s", "value")},
             "plain_loop": plain,
+            "results_equal_alone": {
+                "requests_checked": n_req,
+                "mismatched_vs_plain_loop": same_results(out_served,
+                                                         out_other),
+                "mismatched_vs_march_server": march_mismatched},
             "speedup_solves": served["solves_per_s"] / plain["solves_per_s"],
             "p99_ratio_plain_over_served": plain["p99_ms"] / served["p99_ms"]}
 
@@ -338,11 +369,22 @@ def diffusion2d_leg(B, torch, stream, side_n=16384, count=50, reps=4):
     return out
 
 
+CONFIG = {"workload": "diffusion3d 512^3 FP32, 200 steps per RunKernel",
+          "grid": [N_SIDE, N_SIDE, N_SIDE], "count": COUNT,
+          "input": "analytic sinusoid (t=0) + seeded U[0,1e-3) noise",
+          "l2": "inputs larger than L2 (512 MiB per buffer)"}
+
+
 def run_reference_arm(args):
+    """The reference's own Diffusion3DOpenMP::RunKernel(200) on the 512^3
+    field (oracle/_ref, compiled from the reference sources; the C
+    restatement when that is absent), every timed step one whole
+    RunKernel(200), all host threads.  Rank 0 only."""
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
     import oracle as O
+    from benchmarks_b200.workloads import field_noise
     if not os.path.exists(O.LIB_PATH) or (
             not O.ref_available() and os.path.isdir(O.REF_SRC)):
         O.build()
@@ -350,41 +392,43 @@ def run_reference_arm(args):
     O.set_threads(threads)
     kind = "reference" if O.ref_available() else "port"
     n = N_SIDE
-    sample_steps = 10  # bounded sample of the 200-step RunKernel per step
+    c, _ = O.params(n, n, n)
+    fin = O.initialize(n, n, n)
+    fin += field_noise(fin.shape)
 
     def one():
-        t0 = time.perf_counter()
         if kind == "reference":
-            O.ref_run(n, n, n, 0)
-            t_setup = time.perf_counter() - t0
-            t0 = time.perf_counter()
-            O.ref_run(n, n, n, sample_steps)
-            return time.perf_counter() - t0 - t_setup
-        c, _ = O.params(n, n, n)
-        f = O.initialize(n, n, n)
+            # RunKernel(COUNT) alone, timed inside the probe (the
+            # reference's InitializeBenchmark and the field copies excluded)
+            _, _, secs = O.ref_run(n, n, n, COUNT, field=fin, coeff=c,
+                                   want_time=True, want_field=False)
+            return secs
         t0 = time.perf_counter()
-        O.run(f, c, sample_steps)
+        O.run(fin, c, COUNT)
         return time.perf_counter() - t0
 
     for _ in range(args.warmup):
         one()
     times = [one() for _ in range(args.steps)]
     total = sum(times)
-    value = n ** 3 * sample_steps * args.steps / total / 1e9
+    value = float(n) ** 3 * COUNT * args.steps / total / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * total / args.steps * COUNT / sample_steps,
+        "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (reference Initialize, t=0)",
-        "config": {"workload": "diffusion3d 512^3 FP32, 200 steps per "
-                   "RunKernel; each timed step a %d-step sample" % sample_steps,
-                   "grid": [n, n, n], "count": COUNT, "l2": "input 512 MiB > L2"},
+        "dtype": "f32", "data": "synthetic: analytic sinusoid + seeded "
+                                "U[0,1e-3) noise",
+        "config": dict(CONFIG, parallelism="single GPU" if world == 1
+                       else "independent grid per GPU"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
                          "kind": kind,
-                         "sample": "%d^3, %d of the 200 steps per timed step, "
-                                   "Diffusion3DOpenMP::RunKernel, %d threads"
-                                   % (n, sample_steps, threads)},
+                         "sample": "%d^3, RunKernel(%d) per timed step "
+                                   "(Diffusion3DOpenMP%s), %d threads, "
+                                   "%.2f s per step" % (
+                                       n, COUNT, "" if kind == "reference"
+                                       else ", oracle port", threads,
+                                       total / args.steps)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -414,11 +458,11 @@ def run_b200(args):
     coeff = plan.reference_coefficients()
 
     # Config: analytic sinusoid at t=0 plus seeded U[0, 1e-3) noise.
+    from benchmarks_b200.workloads import field_noise
     f1 = plan.empty()
     f2 = plan.empty()
     plan.analytic(f1, 0.0)
-    gen = torch.Generator(device=dev).manual_seed(0xD1FF + rank)
-    f1.add_(torch.rand(f1.shape, device=dev, generator=gen) * 1e-3)
+    f1.add_(torch.from_numpy(field_noise(plan.shape, 0xD1FF + rank)).to(dev))
     init = f1.clone()
 
     def barrier():
@@ -475,6 +519,10 @@ def run_b200(args):
     achieved = algo_bytes / per_launch_s / 1e9
     traffic = profile_traffic("steps_tb2w_512cube_f32.md" if two_step
                               else "step_tma_512cube_f32.md")
+    traffic_from = ("dram__bytes_read.sum + dram__bytes_write.sum per launch "
+                    "of one ncu capture of this kernel on this workload, read "
+                    "from its committed profile summary (not measured in "
+                    "this run)") if traffic else None
 
     # --- side measurements (not the headline) --------------------------
     def rate_of(p, a_, b_, steps):
@@ -497,8 +545,8 @@ def run_b200(args):
         "value": r, "unit": UNIT, "kernel": inf["last_kernel"],
         "effective_hbm_frac": r * 1e9 * BYTES_PER_UPDATE / (peak * 1e9),
         "note": "temporal-blocked effective rate: 8 B per update counted, "
-                "about 3.9 B per update moved (profiles/"
-                "steps_tb2w_512cube_f32.md)",
+                "about 3.9 B per update moved (ncu capture of the fused "
+                "two-step kernel at 512^3)",
         "grid": inf["grid"], "zchunk": inf["launch_zchunk"]}
     pauto.close()
     for k in (2, 3, 4):
@@ -550,26 +598,37 @@ def run_b200(args):
     r64_rate, _ = rate_of(plan64, g1, g2, 2)
     side["fp64"] = {"value": r64_rate, "unit": UNIT,
                     "hbm_frac": r64_rate * 16 / peak}
-    del g1, g2, r64, x1, x2, r32, init
+    del g1, g2, r64, x1, x2, r32
     plan64.close()
     torch.cuda.synchronize()
 
     # --- e2e: RunKernel-style call with pinned host buffers -------------
+    # The host field starts as this workload's input; every call copies it
+    # in, runs RunKernel(200) and copies the result back over it, so after
+    # E calls it must equal E * 200 device steps from the same input.
     host = B.pinned_empty((n, n, n), np.float32)
-    host[...] = 0
+    host[...] = init.cpu().numpy()
     torch.cuda.synchronize()
-    for _ in range(1):
-        plan.run_host(host, a, b, COUNT, coeff, stream)
+    plan.run_host(host, a, b, COUNT, coeff, stream)  # warm-up (graph)
+    e2e_steps = max(1, args.steps // 2)
     barrier()
     t0 = time.perf_counter()
-    for _ in range(max(1, args.steps // 2)):
+    for _ in range(e2e_steps):
         plan.run_host(host, a, b, COUNT, coeff, stream)
     t_e2e = time.perf_counter() - t0
-    e2e_steps = max(1, args.steps // 2)
     t_e2e = max_over_ranks(t_e2e)
+    x1, x2 = init.clone(), torch.empty_like(init)
+    for _ in range(e2e_steps + 1):
+        x1, x2 = plan.run(x1, x2, COUNT, coeff, stream)
+    torch.cuda.synchronize()
+    e2e_equal = bool(np.array_equal(host.view(np.uint32),
+                                    x1.cpu().numpy().view(np.uint32)))
+    del x1, x2
     e2e = {"value": float(n) ** 3 * COUNT * e2e_steps * world / t_e2e / 1e9,
            "unit": UNIT, "h2d_bytes_per_step": n ** 3 * 4,
-           "d2h_bytes_per_step": n ** 3 * 4}
+           "d2h_bytes_per_step": n ** 3 * 4,
+           "calls": e2e_steps,
+           "result_equals_device_run": e2e_equal}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -577,19 +636,16 @@ def run_b200(args):
         "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: analytic sinusoid + seeded U[0,1e-3) noise",
-        "config": {"workload": "diffusion3d 512^3 FP32, 200 steps per "
-                   "RunKernel (fused two-step TMA passes)"
-                   if two_step else "diffusion3d 512^3 FP32, 200 steps per "
-                   "RunKernel (plain single-step TMA z-march kernel; the "
-                   "fused two-step rate is side.auto)",
-                   "grid": [n, n, n], "count": COUNT,
-                   "l2": "inputs larger than L2 (512 MiB per buffer)",
-                   "parallelism": "independent grid per GPU" if world > 1
-                   else "single GPU", "kernel": info},
+        "config": dict(CONFIG, parallelism="independent grid per GPU"
+                       if world > 1 else "single GPU"),
+        "kernel": dict(info, what="fused two-step TMA passes" if two_step
+                       else "plain single-step TMA z-march kernel (the "
+                       "fused two-step rate is side.auto)"),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind,
                      "traffic": traffic,
+                     "traffic_from": traffic_from,
                      "kernel": info["last_kernel"],
                      "updates_per_point_per_launch": updates_per_launch,
                      "algorithmic_bytes_per_launch": algo_bytes,
@@ -605,7 +661,7 @@ def run_b200(args):
         "side": side,
     }
     if not args.no_side and world == 1:
-        del a, b, f1, f2, host
+        del a, b, f1, f2, host, init
         torch.cuda.empty_cache()
         side["batched"] = batched_leg(B, torch)
         torch.cuda.empty_cache()
@@ -638,14 +694,57 @@ def main():
     ap.add_argument("--batch-kind", type=int, default=None,
                     help="with --only-leg batched: one kernel kind for "
                          "every size class instead of the autotuner")
+    ap.add_argument("--only-kernel", default=None,
+                    help="run `--count` steps of one single-grid kernel "
+                         "(tma, generic, tb2, tb3, tb4, step2d; f64_ "
+                         "prefix for FP64) on a --side^3 field (side^2 for "
+                         "step2d) of seeded uniform values and exit: a "
+                         "fixed small case to profile")
+    ap.add_argument("--side", type=int, default=512)
+    ap.add_argument("--count", type=int, default=4)
+    ap.add_argument("--variant", type=int, default=None)
+    ap.add_argument("--zchunk", type=int, default=0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.only_kernel:
+        return run_one_kernel(args)
     if args.only_leg:
         return run_one_leg(args.only_leg, args.batch_kind)
     return run_b200(args)
+
+
+def run_one_kernel(args):
+    """`args.count` steps of one kernel on a seeded field, then exit."""
+    import torch
+    import benchmarks_b200 as B
+    kernels = {"tma": (B.KERNEL_TMA, 1), "generic": (B.KERNEL_GENERIC, 1),
+               "tb2": (B.KERNEL_TB, 2), "tb3": (B.KERNEL_TB, 3),
+               "tb4": (B.KERNEL_TB, 4), "step2d": (B.KERNEL_AUTO, 1)}
+    torch.cuda.set_device(0)
+    name, dtype = args.only_kernel, B.F32
+    if name.startswith("f64_"):
+        name, dtype = name[4:], B.F64
+    kernel, tb = kernels[name]
+    n = args.side
+    if name == "step2d":
+        plan = B.DiffusionPlan((n, n), dtype, kernel, zchunk=args.zchunk)
+    else:
+        plan = B.Plan(n, n, n, dtype, kernel, tb, variant=args.variant,
+                      zchunk=args.zchunk)
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    tdt = torch.float64 if dtype == B.F64 else torch.float32
+    f1 = torch.rand(plan.shape, device="cuda", generator=gen, dtype=tdt)
+    f2 = torch.empty_like(f1)
+    plan.run(f1, f2, args.count)
+    torch.cuda.synchronize()
+    flags = B.check_device_errors()
+    print("kernel case done: %s n=%d (%dD) x %d steps, %s, device flags %d"
+          % (args.only_kernel, n, plan.ndim, args.count,
+             plan.info()["last_kernel"], flags), flush=True)
+    return 1 if flags else 0
 
 
 def run_one_leg(leg, batch_kind=None):

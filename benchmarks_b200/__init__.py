@@ -388,6 +388,10 @@ class DiffusionPlan(Plan):
         return diffusion_coefficients(self.ndim, self.dims, self.dtype)[0]
 
 
+# Kernel kinds of the batch API (d3d_batch_set_kind).
+BATCH_NUM_KINDS = 8
+
+
 class BatchGrid(ctypes.Structure):
     """d3d_batch_grid: one grid of a batch."""
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int),

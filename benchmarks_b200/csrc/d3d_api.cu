@@ -12,6 +12,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "d3d_b200.h"
@@ -54,18 +55,32 @@ int cuda_fail(cudaError_t e, const char* what) {
     if (e__ != cudaSuccess) return cuda_fail(e__, what); \
   } while (0)
 
+// Device address of the error word in the current context, looked up once
+// per context (a cudaDeviceReset replaces the device's primary context, and
+// with it this address).
 unsigned* dev_error_ptr() {
-  static unsigned* ptrs[64] = {nullptr};
+  struct Slot {
+    void* ctx = nullptr;
+    unsigned* ptr = nullptr;
+  };
+  static Slot slots[64];
+  static std::mutex mu;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
     return nullptr;
-  if (!ptrs[dev]) {
+  void* ctx = nullptr;
+  if (d3d::current_context(&ctx) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  Slot& slot = slots[dev];
+  if (!ctx || !slot.ptr || slot.ctx != ctx) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_dev_error_word) != cudaSuccess)
       return nullptr;
-    ptrs[dev] = static_cast<unsigned*>(p);
+    if (d3d::current_context(&ctx) != cudaSuccess) return nullptr;
+    slot.ptr = static_cast<unsigned*>(p);
+    slot.ctx = ctx;
   }
-  return ptrs[dev];
+  return slot.ptr;
 }
 
 cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
@@ -865,10 +880,18 @@ int d3d_compare_noalloc(const void* a, int a_dtype, const void* b,
                 "n = %zu exceeds the allocation-free limit of %zu elements "
                 "(use d3d_compare for larger fields)",
                 n, max_n);
+  cudaStream_t s = as_stream(stream);
+  // The report comes back to the host, so the call waits for its stream;
+  // a stream that is being captured cannot be waited for.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  D3D_TRY(cudaStreamIsCapturing(s, &cap), "cudaStreamIsCapturing");
+  if (cap != cudaStreamCaptureStatusNone)
+    return fail(D3D_E_INVALID,
+                "d3d_compare_noalloc waits for its stream and cannot be "
+                "called on a stream that is being captured");
   double* scratch = nullptr;
   D3D_TRY(d3d::noalloc_scratch(&scratch),
           "cudaGetSymbolAddress (allocation-free scratch)");
-  cudaStream_t s = as_stream(stream);
   D3D_TRY(d3d::launch_compare_noalloc(a, a_dtype, b, b_dtype, n, scratch, s),
           "compare launch");
   g_launches.fetch_add(n ? 2 : 1, std::memory_order_relaxed);

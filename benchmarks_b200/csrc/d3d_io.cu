@@ -209,6 +209,14 @@ int checkpoint_load(const PlanShape& ps, double* scratch, const char* path,
                      path, h.ndim, h.nx, h.ny, h.nz,
                      h.dtype ? "FP64" : "FP32", ps.ndim, ps.nx, ps.ny, ps.nz,
                      ps.dtype ? "FP64" : "FP32");
+  // Bit 0 of flags: the field is in the diffusion::Diffusion surface's
+  // order.  Same shape, other surface: refused, not silently reordered.
+  if ((h.flags & 1u) != (ps.flip_y ? 1u : 0u))
+    return set_error(D3D_E_INVALID,
+                     "%s was saved from a %s plan; this plan is a %s plan",
+                     path, (h.flags & 1u) ? "diffusion::Diffusion"
+                                          : "diffusion3d",
+                     ps.flip_y ? "diffusion::Diffusion" : "diffusion3d");
   const size_t total = h.payload;
   const size_t chunk = std::min(kChunk, std::max<size_t>(total, 1));
   Staging st;

@@ -213,6 +213,11 @@ cudaError_t launch_repitch(const float* src, float* dst, int nx, int px,
 // This device's kernel error word (bounded-wait failures).
 unsigned* device_error_word();
 
+// The driver context current on the calling thread (null when the runtime
+// has not made one current yet).  Device addresses of file-scope
+// __device__ variables are cached per context with it.
+cudaError_t current_context(void** ctx);
+
 // Tile shapes of the multi-grid step kernel (256 threads each).
 struct BShape {
   int bx, by;

@@ -8,8 +8,8 @@
 //   * compare kernels  -- rms, max-abs, max-rel and a checksum accumulated
 //     in double over two device fields of any dtype pair, in a fixed
 //     reduction order (deterministic for a given device).
-#include <atomic>
 #include <cfloat>
+#include <mutex>
 
 #include "d3d_common.cuh"
 #include "d3d_kernels.h"
@@ -30,10 +30,17 @@ struct Acc {
   double ss, mx, mr, sa;
 };
 
+// max that keeps a NaN: fmax returns the other operand when one is NaN,
+// which would report a finite max_abs / max_rel for a field holding NaNs
+// (its rms and checksum are NaN already).
+__device__ __forceinline__ double nan_max(double a, double b) {
+  return (isnan(a) || isnan(b)) ? a + b : fmax(a, b);
+}
+
 __device__ __forceinline__ void acc_merge(Acc& a, const Acc& b) {
   a.ss += b.ss;
-  a.mx = fmax(a.mx, b.mx);
-  a.mr = fmax(a.mr, b.mr);
+  a.mx = nan_max(a.mx, b.mx);
+  a.mr = nan_max(a.mr, b.mr);
   a.sa += b.sa;
 }
 
@@ -72,8 +79,8 @@ __global__ void __launch_bounds__(kCmpThreads)
     const double ad = fabs(d);
     const double den = fmax(fabs(y), 1e-300);
     v.ss += d * d;
-    v.mx = fmax(v.mx, ad);
-    v.mr = fmax(v.mr, ad / den);
+    v.mx = nan_max(v.mx, ad);
+    v.mr = nan_max(v.mr, ad / den);
     v.sa += x;
   }
   Acc r = block_reduce(v);
@@ -144,8 +151,8 @@ __global__ void __launch_bounds__(kCmpThreads)
     const double d = x - y_ref;
     const double ad = fabs(d);
     v.ss += d * d;
-    v.mx = fmax(v.mx, ad);
-    v.mr = fmax(v.mr, ad / fmax(fabs(y_ref), 1e-300));
+    v.mx = nan_max(v.mx, ad);
+    v.mr = nan_max(v.mr, ad / fmax(fabs(y_ref), 1e-300));
     v.sa += x;
   }
   Acc r = block_reduce(v);
@@ -192,11 +199,10 @@ cudaError_t launch_partial(const void* a, const void* b, int b_dtype, size_t n,
 // Some callers cannot allocate device memory when they need the error
 // report: a serving process that has already handed all free HBM to its
 // solve arena, a host whose allocator policy forbids driver allocations
-// behind its back, or code inside a global-mode stream capture, where
-// cudaMalloc is not permitted (and, outside capture, cudaMalloc would
-// synchronise the device in the middle of a latency-sensitive loop).  For
-// them the partial sums live in this fixed file-scope array, which every
-// GPU that loads the library holds until the process exits.
+// behind its back, or a latency-sensitive loop in which a cudaMalloc would
+// synchronise the whole device.  For them the partial sums live in this
+// fixed file-scope array, which every GPU that loads the library holds
+// until the process exits.
 //
 // Limits and sharing: one partial per kNoAllocChunk elements, at most
 // kNoAllocMaxParts partials, so n <= 2^28 elements (1 GiB of FP32).  Every
@@ -222,8 +228,8 @@ __global__ void __launch_bounds__(kCmpThreads)
     const double d = x - y;
     const double ad = fabs(d);
     v.ss += d * d;
-    v.mx = fmax(v.mx, ad);
-    v.mr = fmax(v.mr, ad / fmax(fabs(y), 1e-300));
+    v.mx = nan_max(v.mx, ad);
+    v.mr = nan_max(v.mr, ad / fmax(fabs(y), 1e-300));
     v.sa += x;
   }
   Acc r = block_reduce(v);
@@ -253,25 +259,41 @@ size_t compare_noalloc_max_elements() {
   return (size_t)kNoAllocMaxParts * kNoAllocChunk;
 }
 
-// Device address of g_noalloc_scratch on the current device.  Looked up
-// once per device (the first allocation-free call on that device) with
-// that device current; in host code the array's name is only a host-side
-// stand-in, never a device address.
+// Device address of g_noalloc_scratch in the current device's context.
+// In host code the array's name is only a host-side stand-in, never a
+// device address, so the address is looked up with cudaGetSymbolAddress,
+// with the device current, the first time a context of that device calls
+// this (once per device, and once more after a cudaDeviceReset has
+// replaced the device's primary context: the lookup is keyed on the
+// context, so an address from a destroyed context is never reused).
 cudaError_t noalloc_scratch(double** out) {
-  static std::atomic<double*> cache[64];
+  struct Slot {
+    void* ctx = nullptr;
+    double* ptr = nullptr;
+  };
+  static Slot cache[64];
+  static std::mutex mu;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  double* p = cache[dev].load();
-  if (!p) {
+  void* ctx = nullptr;
+  e = current_context(&ctx);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  Slot& slot = cache[dev];
+  if (!ctx || !slot.ptr || slot.ctx != ctx) {
+    // (No context current yet: the lookup itself makes the device's
+    // primary context current.)
     void* addr = nullptr;
     e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
-    p = static_cast<double*>(addr);
-    cache[dev].store(p);
+    e = current_context(&ctx);
+    if (e != cudaSuccess) return e;
+    slot.ptr = static_cast<double*>(addr);
+    slot.ctx = ctx;
   }
-  *out = p;
+  *out = slot.ptr;
   return cudaSuccess;
 }
 

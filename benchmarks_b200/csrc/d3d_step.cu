@@ -283,6 +283,30 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+
+}  // namespace
+
+cudaError_t current_context(void** ctx) {
+  static CtxGetCurrentFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault,
+                                &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      return reinterpret_cast<CtxGetCurrentFn>(p);
+    return static_cast<CtxGetCurrentFn>(nullptr);
+  }();
+  *ctx = nullptr;
+  if (!fn) return cudaErrorNotSupported;
+  CUcontext c = nullptr;
+  if (fn(&c) != CUDA_SUCCESS) return cudaErrorInvalidContext;
+  *ctx = c;
+  return cudaSuccess;
+}
+
+namespace {
+
 int num_sms() {
   int dev = 0, n = 0;
   cudaGetDevice(&dev);

@@ -4,7 +4,7 @@
 // Two additions: --kernel {auto,generic,tb2,tb3,tb4} picks the B200 kernel,
 // and --dump-binary dumps a binary checkpoint instead of the text.
 // In the reference tree the same selection is one more branch of main.cc's
-// variant chain.
+// variant chain: `#elif defined(CUDA_B200)` creating a Diffusion3DB200.
 #include <getopt.h>
 #include <stdlib.h>
 #include <string.h>

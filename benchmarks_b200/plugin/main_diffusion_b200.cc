@@ -4,7 +4,8 @@
 // nd sides of --size.  Two additions: --kernel {auto,generic,tb2,tb3,tb4}
 // picks the B200 kernel (tb* in 3D only), and --dump-binary dumps a binary
 // checkpoint instead of the text.  In the reference tree the same
-// selection is one more branch of main.cc's variant chain.
+// selection is one more branch of main.cc's variant chain, creating a
+// DiffusionB200.
 #include <assert.h>
 #include <getopt.h>
 #include <stdlib.h>

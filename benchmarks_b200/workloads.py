@@ -7,6 +7,8 @@
 * ``serving_requests`` -- a Poisson request stream (mean rate `rate`/s) of
   cubic grids with sides log-uniform in [32, 256] and step counts
   log-uniform in [10, 2000].
+* ``field_noise`` -- the seeded U[0, 1e-3) noise added to the analytic
+  initial field of the single-grid workload (512^3, 200 steps).
 
 No public dataset is involved; the reference has none for this path.
 """
@@ -41,3 +43,11 @@ def serving_requests(n=256, seed=0x5E7F, rate=2000.0, side=(32, 256),
     sts = np.exp(rng.uniform(math.log(steps[0]), math.log(steps[1]), n))
     return [(float(a), int(round(s)), int(round(k)))
             for a, s, k in zip(t, sides, sts)]
+
+
+def field_noise(shape, seed=0xD1FF, amplitude=1e-3):
+    """Seeded U[0, amplitude) FP32 noise of `shape` (numpy, host)."""
+    rng = np.random.default_rng(seed)
+    noise = rng.random(shape, dtype=np.float32)
+    noise *= np.float32(amplitude)
+    return noise

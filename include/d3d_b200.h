@@ -185,9 +185,12 @@ int d3d_analytic(d3d_plan plan, void* out, double time, void* stream);
  * payload's 32-bit words modulo 2^64, payload bytes, surface flag) and the
  * raw field, x fastest (benchmarks_b200.read_checkpoint reads one on a
  * host).  Device copies go through pinned staging that overlaps PCIe and
- * file I/O.  Load checks the shape and dtype against the plan
- * (D3D_E_INVALID) and the stored checksum against the loaded field
- * (D3D_E_IO); *step (may be NULL) receives the saved step.  The device
+ * file I/O.  Load checks the shape, dtype and surface flag against the
+ * plan (D3D_E_INVALID, before the field is touched) and the stored checksum
+ * against the loaded field (D3D_E_IO); *step (may be NULL) receives the
+ * saved step.  A load that fails after the header checks (a truncated or
+ * corrupt payload, D3D_E_IO) leaves `field` partly overwritten: its
+ * contents are then undefined.  The device
  * forms synchronise `stream`; d3d_checkpoint_save_host writes the same file
  * from a field in host memory (what a plugin's Dump holds in f1_). */
 int d3d_checkpoint_save(d3d_plan plan, const void* field, long long step,
@@ -357,22 +360,25 @@ int d3d_server_destroy(d3d_server server);
 /* d3d_compare without any device allocation.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory at
  * the moment they want an error report -- a serving loop that has already
- * given all free HBM to its solve arena, a host whose allocator policy
- * forbids driver allocations behind its back, or code inside a global-mode
- * stream capture (where cudaMalloc is not allowed; outside capture it would
- * also synchronise the device mid-loop).  The caller still passes the two
- * fields; the partial sums go to a fixed 128 KiB array in the library's
- * device image, which every GPU that loads the library keeps until exit.
+ * given all free HBM to its solve arena, or a host whose allocator policy
+ * forbids driver allocations behind its back (a cudaMalloc would also
+ * synchronise the whole device in the middle of a latency-sensitive loop).
+ * The caller still passes the two fields; the partial sums go to a fixed
+ * 128 KiB array in the library's device image, which every GPU that loads
+ * the library keeps until exit.
  *  - n may be at most D3D_NOALLOC_MAX_ELEMENTS (2^28 elements, 1 GiB of
  *    FP32); larger n returns D3D_E_INVALID without touching the GPU.
- *  - The first call on a device looks up the array's device address (once
- *    per device, that device current); make that first call before any
- *    stream capture.
+ *  - The first call in a device's context looks up the array's device
+ *    address (once per device, that device current; again after a
+ *    cudaDeviceReset).
  *  - All calls share the array.  Each call writes every slot it reads, so
  *    results never depend on an earlier call, but calls whose kernels
  *    overlap on the GPU (different streams with no ordering) race.
+ *  - The report is copied back to `out` on the host, so the call waits for
+ *    `stream`; on a stream that is being captured it returns D3D_E_INVALID
+ *    before launching anything.
  * Same outputs as d3d_compare (summation order differs: sums agree to
- * rounding, maxima exactly).  Synchronises `stream`. */
+ * rounding, maxima exactly; a NaN in either field makes every output NaN). */
 #define D3D_NOALLOC_MAX_ELEMENTS ((size_t)1 << 28)
 int d3d_compare_noalloc(const void* a, int a_dtype, const void* b,
                         int b_dtype, size_t n, double out[4], void* stream);

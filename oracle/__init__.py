@@ -29,7 +29,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_LIB_PATH = os.path.join(HERE, "_ref", "libd3d_ref.so")
 DIF_REF_LIB_PATH = os.path.join(HERE, "_ref", "libdif_ref.so")
-REF_SRC = "/root/reference/src"
+# Where the reference's sources lie (its src/ directory).  Only the build
+# recipe (oracle/Makefile, `make ref`) and the tests that rebuild it read
+# them; machines without the tree use what was built beforehand.
+REF_SRC = os.environ.get("D3D_REFERENCE_SRC", "/root/reference/src")
 
 _f32p = ctypes.POINTER(ctypes.c_float)
 _f64p = ctypes.POINTER(ctypes.c_double)
@@ -48,7 +51,8 @@ def build(with_ref: bool | None = None) -> None:
     if with_ref is None:
         with_ref = os.path.isdir(REF_SRC)
     targets = ["all"] + (["ref"] if with_ref else [])
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "REF_SRC=" + REF_SRC]
+                   + targets, check=True)
 
 
 def lib():
@@ -102,6 +106,10 @@ def ref():
         R = ctypes.CDLL(REF_LIB_PATH)
         R.d3dref_run.argtypes = ([ctypes.c_int] * 4 + [_f32p, _f32p, _f32p,
                                  ctypes.c_int, _f32p, ctypes.c_int])
+        R.d3dref_run_timed.argtypes = (
+            [ctypes.c_int] * 4 + [_f32p, _f32p, _f32p, ctypes.c_int, _f32p,
+                                  ctypes.c_int,
+                                  ctypes.POINTER(ctypes.c_double)])
         R.d3dref_params.argtypes = [ctypes.c_int] * 3 + [_f32p, _f32p]
         R.d3dref_initialize.argtypes = ([_f32p] + [ctypes.c_int] * 3
                                         + [ctypes.c_float] * 8)
@@ -207,21 +215,24 @@ def ref_initialize(nx, ny, nz, time=0.0):
 
 
 def ref_run(nx, ny, nz, count, field=None, coeff=None, backend=REF_OPENMP,
-            want_accuracy=False):
-    """Runs the reference backend; returns (field after count steps, acc)."""
-    out = np.empty((nz, ny, nx), np.float32)
+            want_accuracy=False, want_time=False, want_field=True):
+    """Runs the reference backend; returns (field after count steps, acc),
+    plus the seconds RunKernel(count) alone took when want_time."""
+    out = np.empty((nz, ny, nx), np.float32) if want_field else None
     acc = np.zeros(1, np.float32)
+    secs = ctypes.c_double(0.0)
     fin = None if field is None else np.ascontiguousarray(field, np.float32)
     cin = None if coeff is None else np.ascontiguousarray(coeff, np.float32)
-    rc = ref().d3dref_run(
+    rc = ref().d3dref_run_timed(
         backend, nx, ny, nz,
         None if cin is None else _ptr(cin, _f32p),
         None if fin is None else _ptr(fin, _f32p),
-        _ptr(out, _f32p), count,
-        _ptr(acc, _f32p) if want_accuracy else None, 0)
+        None if out is None else _ptr(out, _f32p), count,
+        _ptr(acc, _f32p) if want_accuracy else None, 0, ctypes.byref(secs))
     if rc != 0:
         raise RuntimeError("d3dref_run failed: %d" % rc)
-    return out, (float(acc[0]) if want_accuracy else None)
+    res = (out, (float(acc[0]) if want_accuracy else None))
+    return res + (secs.value,) if want_time else res
 
 
 def ref_rates(nx, ny, nz, count, time):

@@ -14,6 +14,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <chrono>
+
 #include "diffusion3d/baseline.h"
 #include "diffusion3d/diffusion3d_openmp.h"
 #include "diffusion3d/diffusion3d_openmp_temporal_blocking.h"
@@ -60,12 +62,18 @@ class Probe : public Backend {
 
 template <class Backend>
 int RunProbe(int nx, int ny, int nz, const float *coeff, const float *in,
-             float *out, int count, float *accuracy, int dump) {
+             float *out, int count, float *accuracy, int dump,
+             double *run_seconds) {
   Probe<Backend> p(nx, ny, nz);
   p.Setup();
   if (coeff) p.SetCoeffs(coeff);
   if (in) p.SetField(in);
+  const auto t0 = std::chrono::steady_clock::now();
   p.Run(count);
+  if (run_seconds)
+    *run_seconds = std::chrono::duration<double>(
+                       std::chrono::steady_clock::now() - t0)
+                       .count();
   if (out) p.GetField(out);
   if (accuracy) *accuracy = p.Accuracy(count);
   if (dump) p.DumpField();
@@ -80,23 +88,32 @@ extern "C" {
 // Runs `count` steps of the chosen reference backend.  `coeff` (7 floats,
 // ce..cc) and `in` (nx*ny*nz floats) are optional overrides of what the
 // reference's own constructor and InitializeBenchmark produce.  The field
-// after `count` steps (the reference's f1_) lands in `out` when non-null.
-int d3dref_run(int backend, int nx, int ny, int nz, const float *coeff,
-               const float *in, float *out, int count, float *accuracy,
-               int dump) {
+// after `count` steps (the reference's f1_) lands in `out` when non-null;
+// `run_seconds`, when non-null, receives the wall time of RunKernel(count)
+// alone (InitializeBenchmark and the copies excluded).
+int d3dref_run_timed(int backend, int nx, int ny, int nz, const float *coeff,
+                     const float *in, float *out, int count, float *accuracy,
+                     int dump, double *run_seconds) {
   switch (backend) {
     case 0:
       return RunProbe<Diffusion3DOpenMP>(nx, ny, nz, coeff, in, out, count,
-                                         accuracy, dump);
+                                         accuracy, dump, run_seconds);
     case 1:
       return RunProbe<Baseline>(nx, ny, nz, coeff, in, out, count, accuracy,
-                                dump);
+                                dump, run_seconds);
     case 2:
       return RunProbe<Diffusion3DOpenMPTemporalBlocking>(
-          nx, ny, nz, coeff, in, out, count, accuracy, dump);
+          nx, ny, nz, coeff, in, out, count, accuracy, dump, run_seconds);
     default:
       return -1;
   }
+}
+
+int d3dref_run(int backend, int nx, int ny, int nz, const float *coeff,
+               const float *in, float *out, int count, float *accuracy,
+               int dump) {
+  return d3dref_run_timed(backend, nx, ny, nz, coeff, in, out, count,
+                          accuracy, dump, nullptr);
 }
 
 // The reference constructor's derived quantities for an nx*ny*nz grid.

@@ -117,6 +117,15 @@ def test_device_load_rejects_wrong_shape_and_damage(tmp_path):
     with pytest.raises(B.D3DError) as ei:
         plan.load_checkpoint(str(tmp_path / "missing.d3d"), buf)
     assert ei.value.code == B.D3D_E_IO
+    # Same shape, saved from the diffusion::Diffusion surface (y order
+    # flipped): refused before the field is touched.
+    B.write_checkpoint(p, a, diffusion_surface=True)
+    buf.fill_(7.0)
+    with pytest.raises(B.D3DError) as ei:
+        plan.load_checkpoint(p, buf)
+    assert ei.value.code == B.D3D_E_INVALID
+    assert "diffusion::Diffusion" in str(ei.value)
+    assert bool((buf == 7.0).all())
     assert B.check_device_errors() == 0
     plan.close()
 

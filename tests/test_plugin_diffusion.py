@@ -125,7 +125,7 @@ def test_standalone_driver_builds():
                     reason="reference tree not present")
 def test_dropin_builds_against_reference_headers():
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"),
-                    "dropin"], check=True)
+                    "REF_SRC=" + O.REF_SRC, "dropin"], check=True)
     assert os.path.exists(DROPIN)
 
 
