@@ -300,7 +300,7 @@ cudaError_t current_context(void** ctx) {
   *ctx = nullptr;
   if (!fn) return cudaErrorNotSupported;
   CUcontext c = nullptr;
-  if (fn(&c) != CUDA_SUCCESS) return cudaErrorInvalidContext;
+  if (fn(&c) != CUDA_SUCCESS) return cudaErrorDeviceUninitialized;
   *ctx = c;
   return cudaSuccess;
 }
