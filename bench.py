@@ -332,6 +332,54 @@ def serving_leg(B, torch, n_req=256, arena_gb=24.0, chunk=8):
             "p99_ratio_plain_over_served": plain["p99_ms"] / served["p99_ms"]}
 
 
+def slab_leg(B, torch, dist, side_n=1024, count=20):
+    """One side_n^3 FP32 grid split into z slabs across the ranks (the
+    overlapped schedule: boundary planes first, their exchange over NCCL
+    while the interior steps); Gpt-updates/s of the whole grid, device time
+    from CUDA events, max over ranks.  At one rank there is no exchange."""
+    from benchmarks_b200.distributed import SingleProcess, SlabSolver
+    group = dist if dist is not None else SingleProcess()
+    c = B.coefficients(side_n, side_n, side_n)[0]
+    solver = SlabSolver(group, side_n, side_n, side_n, c, halo=1,
+                        overlap=True)
+    d = solver.dec
+    # The analytic initial field on this rank's planes (ghosts included).
+    dev = solver.f1.device
+    two_pi = 2.0 * 3.141592653589793
+
+    def factor(lo, hi, n):
+        i = torch.arange(lo, hi, device=dev, dtype=torch.float64)
+        return 1.0 - torch.cos(two_pi * (i + 0.5) / n)
+    f = (0.125 * factor(d.lo, d.hi, side_n)[:, None, None]
+         * factor(0, side_n, side_n)[None, :, None]
+         * factor(0, side_n, side_n)[None, None, :])
+    solver.f1.copy_(f.float())
+    del f
+    solver.run(2)  # warm-up
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    solver.run(count)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    solver.close()
+    del solver
+    torch.cuda.empty_cache()
+    return {"grid": [side_n] * 3, "steps": count, "ranks": d.world,
+            "schedule": "overlapped, halo 1 (d3d_step_planes + NCCL "
+                        "send/recv of one plane per neighbour per step)",
+            "ms": ms, "value": float(side_n) ** 3 * count / (ms / 1e3) / 1e9,
+            "unit": UNIT, "scaling": "strong"}
+
+
 def diffusion2d_leg(B, torch, stream, side_n=16384, count=50, reps=4):
     """The second plugin surface's 2D 5-point grid (diffusion::Diffusion,
     nd = 2): device rate of the register-march kernel at side_n^2 (1 GiB
@@ -660,6 +708,9 @@ def run_b200(args):
         "correctness": report,
         "side": side,
     }
+    if not args.no_side:
+        # Every rank takes part (the exchange is a collective step).
+        side["slab"] = slab_leg(B, torch, dist)
     if not args.no_side and world == 1:
         del a, b, f1, f2, host, init
         torch.cuda.empty_cache()

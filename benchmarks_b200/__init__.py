@@ -56,6 +56,7 @@ _SIGNATURES = {
     "d3d_memcpy": ([_vp, _vp, _sz, _vp], _i),
     "d3d_stream_sync": ([_vp], _i),
     "d3d_step": ([_vp, _vp, _vp, _vp, _vp], _i),
+    "d3d_step_planes": ([_vp, _vp, _vp, _i, _i, _vp, _vp], _i),
     "d3d_run": ([_vp, _vpp, _vpp, _vp, _i, _vp], _i),
     "d3d_run_host": ([_vp, _vp, _vp, _vp, _vp, _i, _vp,
                       ctypes.POINTER(ctypes.c_float)], _i),
@@ -78,6 +79,7 @@ _SIGNATURES = {
     "d3d_batch_set_kind": ([_vp, _i], _i),
     "d3d_batch_run": ([_vp, _vp, ctypes.POINTER(ctypes.c_float)], _i),
     "d3d_batch_info": ([_vp, ctypes.c_char_p, _sz], _i),
+    "d3d_batch_progress": ([_vp, ctypes.POINTER(ctypes.c_int), _i], _i),
     "d3d_batch_destroy": ([_vp], _i),
     "d3d_server_create": ([_sz, _i, _vpp], _i),
     "d3d_server_submit": ([_vp, _i, _i, _i, _i,
@@ -279,6 +281,15 @@ class Plan:
         check(lib().d3d_step(self._h, f1.data_ptr(), f2.data_ptr(),
                              c.ctypes.data, _stream_handle(stream)))
 
+    def step_planes(self, f1, f2, z_begin, z_end, coeff=None, stream=None):
+        """One step of output planes [z_begin, z_end) (d3d_step_planes)."""
+        self._check_buf(f1)
+        self._check_buf(f2)
+        c = self._coeff(coeff)
+        check(lib().d3d_step_planes(self._h, f1.data_ptr(), f2.data_ptr(),
+                                    int(z_begin), int(z_end), c.ctypes.data,
+                                    _stream_handle(stream)))
+
     def run(self, f1, f2, count, coeff=None, stream=None):
         """`count` steps ping-ponging f1/f2; returns (result, other)."""
         self._check_buf(f1)
@@ -388,8 +399,10 @@ class DiffusionPlan(Plan):
         return diffusion_coefficients(self.ndim, self.dims, self.dtype)[0]
 
 
-# Kernel kinds of the batch API (d3d_batch_set_kind).
-BATCH_NUM_KINDS = 8
+# Kernel kinds of the batch API (d3d_batch_set_kind); kind 8 is the
+# cluster-resident kernel for every grid it fits.
+BATCH_NUM_KINDS = 9
+BATCH_KIND_RESIDENT = 8
 
 
 class BatchGrid(ctypes.Structure):
@@ -466,7 +479,8 @@ class Batch:
     def set_kind(self, kind):
         """Every size class to one kernel kind: 0..3 the march kernel's
         tile shapes, 4 and 5 the strip kernel (4 is the default), 6 and 7
-        its two-step form (grids at most 248 floats wide)."""
+        its two-step form (grids at most 248 floats wide), 8 the
+        cluster-resident kernel for every grid it fits."""
         check(lib().d3d_batch_set_kind(self._h, int(kind)))
 
     def run(self, stream=None, timed=True):
@@ -477,9 +491,17 @@ class Batch:
 
     def info(self):
         import json
-        buf = ctypes.create_string_buffer(4096)
+        buf = ctypes.create_string_buffer(16384)
         check(lib().d3d_batch_info(self._h, buf, len(buf)))
         return json.loads(buf.value.decode())
+
+    def progress(self):
+        """Per-grid step counters of the last run (d3d_batch_progress)."""
+        out = np.zeros(len(self.grids), np.int32)
+        check(lib().d3d_batch_progress(
+            self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+            len(out)))
+        return out
 
     def close(self):
         if getattr(self, "_h", None):

@@ -228,7 +228,7 @@ int check_device(d3d_plan p) {
 
 // One single-step launch, choosing the TMA path when the buffer allows it.
 int step_once(d3d_plan p, const void* f1, void* f2, const void* coeff,
-              cudaStream_t s) {
+              cudaStream_t s, int zb = 0, int ze = -1) {
   if (p->ndim == 2) {
     D3D_TRY(d3d::launch_step2d(f1, f2, p->nx, p->ny, coeff, p->dtype,
                                p->variant, p->zchunk, s, &p->last),
@@ -250,12 +250,13 @@ int step_once(d3d_plan p, const void* f1, void* f2, const void* coeff,
     if (rc) return rc;
     D3D_TRY(d3d::launch_step_tma(*map, f2, p->nx, p->ny, p->nz, coeff,
                                  p->dtype, p->variant, p->zchunk, p->flip_y,
-                                 s, dev_error_ptr(), &p->last),
+                                 s, dev_error_ptr(), &p->last, zb, ze),
             "step_tma launch");
     p->last_kernel = "step_tma";
   } else {
     D3D_TRY(d3d::launch_step_generic(f1, f2, p->nx, p->ny, p->nz, coeff,
-                                     p->dtype, p->flip_y, s, &p->last),
+                                     p->dtype, p->flip_y, s, &p->last, zb,
+                                     ze),
             "step_generic launch");
     p->last_kernel = "step_generic";
   }
@@ -709,6 +710,20 @@ int d3d_step(d3d_plan p, const void* f1, void* f2, const void* coeff,
   int rc = check_device(p);
   if (rc) return rc;
   return step_once(p, f1, f2, coeff, as_stream(stream));
+}
+
+int d3d_step_planes(d3d_plan p, const void* f1, void* f2, int z_begin,
+                    int z_end, const void* coeff, void* stream) {
+  if (!p || !f1 || !f2 || !coeff) return fail(D3D_E_INVALID, "NULL argument");
+  if (f1 == f2) return fail(D3D_E_INVALID, "f1 and f2 alias");
+  if (p->ndim != 3)
+    return fail(D3D_E_UNSUPPORTED, "plane ranges are for 3D plans");
+  if (z_begin < 0 || z_begin >= z_end || z_end > p->nz)
+    return fail(D3D_E_INVALID, "planes [%d, %d) outside [0, %d)", z_begin,
+                z_end, p->nz);
+  int rc = check_device(p);
+  if (rc) return rc;
+  return step_once(p, f1, f2, coeff, as_stream(stream), z_begin, z_end);
 }
 
 int d3d_run(d3d_plan p, void** f1, void** f2, const void* coeff, int count,

@@ -110,7 +110,10 @@ int class_of(int nx) {
 // d3d::kStripMaxW floats wide.
 constexpr int kStripKind = kNumBShapes;
 constexpr int kStrip2Kind = kStripKind + 2;
-constexpr int kNumKinds = kStrip2Kind + 2;
+// Kind 8 is batch-wide: every grid that fits runs on the cluster-resident
+// kernel (d3d_resident.cu); the rest keep per-class kinds 0..7.
+constexpr int kResidentKind = kStrip2Kind + 2;
+constexpr int kNumKinds = kResidentKind + 1;
 constexpr int kDefaultKind = kStripKind;  // before the autotuner runs
 int kind_nr(int kind) {
   return kind >= kStrip2Kind ? kind - kStrip2Kind + 1
@@ -118,6 +121,17 @@ int kind_nr(int kind) {
                               : 0;
 }
 bool kind_two(int kind) { return kind >= kStrip2Kind; }
+
+// One launch of the cluster-resident kernel: grids of one cluster size and
+// thread shape, largest work first.
+struct ResidentClass {
+  int cluster = 1, variant = 0, nclusters = 0;
+  size_t smem = 0;
+  std::vector<int> grids;
+  d3d::ResidentDesc* d_descs = nullptr;
+  unsigned* d_queue = nullptr;
+};
+constexpr int kSideStreams = 4;
 
 struct ClassPlan {
   std::vector<int> grids;  // batch indices, sorted by steps descending
@@ -157,6 +171,20 @@ struct d3d_batch_s {
   int device = 0;
   long long total_items = 0;
   unsigned long long launches_per_run = 0;
+  // Cluster-resident kernel: which grids fit it, whether it is in use, its
+  // launches, the per-grid step counters, and the side streams its
+  // launches run on (forked from and joined back to the run's stream).
+  std::vector<char> resident_ok;
+  std::vector<d3d::ResidentDesc> rdesc;  // per grid (resident_ok ones)
+  std::vector<int> rclass_of;            // per grid: index into rclasses
+  std::vector<ResidentClass> rclasses;
+  bool resident_on = false;
+  int* d_counters = nullptr;
+  int2* d_classic_steps = nullptr;  // (grid, steps) of the per-step grids
+  int n_classic = 0;
+  cudaStream_t side[kSideStreams] = {};
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join[kSideStreams] = {};
 };
 
 namespace {
@@ -418,6 +446,214 @@ void drop_graph(d3d_batch b) {
   b->exec = nullptr;
 }
 
+// Which grids fit the cluster-resident kernel, and its launch classes:
+// a grid with S = ceil(nx/4) row segments fits when a thread shape covers
+// its S * ny segments a plane and a cluster of at most 16 CTAs holds its
+// nz planes, pc a CTA plus one halo plane, in the shared memory a CTA may
+// have.  Grids with 0 steps are their own result and never run.
+int plan_resident(d3d_batch b) {
+  const int n = (int)b->grids.size();
+  b->resident_ok.assign(n, 0);
+  b->rdesc.assign(n, d3d::ResidentDesc{});
+  b->rclass_of.assign(n, -1);
+  b->rclasses.clear();
+  cudaError_t e = d3d::resident_prepare();
+  if (e != cudaSuccess) {
+    // Without the kernel's attributes every grid keeps the per-step kinds.
+    cudaGetLastError();
+    return D3D_OK;
+  }
+  const size_t cap = d3d::kResidentSmemMax / 4;  // floats a CTA may hold
+  std::vector<std::pair<int, int>> keys;          // (cluster, variant)
+  for (int i = 0; i < n; ++i) {
+    const d3d_batch_grid& g = b->grids[i];
+    if (g.steps < 1) continue;
+    const int px = pitch_of(g.nx), segs = px / 4;
+    const long long plane = (long long)px * g.ny;
+    const long long units = (long long)segs * g.ny;
+    int v = -1;
+    for (int j = 0; j < d3d::kNumResidentVariants && v < 0; ++j) {
+      const d3d::ResidentVariant& rv = d3d::resident_variant(j);
+      if (units <= (long long)rv.threads * rv.units) v = j;
+    }
+    if (v < 0) continue;
+    const long long pmax = (long long)cap / plane - 1;
+    if (pmax < 1) continue;
+    const int cl = (int)((g.nz + pmax - 1) / pmax);
+    if (cl > d3d::kResidentMaxCluster) continue;
+    const int pc = (g.nz + cl - 1) / cl;
+    d3d::ResidentDesc& d = b->rdesc[i];
+    d.in = b->arena + g.offset_a;
+    d.out = b->arena + ((g.steps & 1) ? g.offset_b : g.offset_a);
+    d.nx = g.nx;
+    d.ny = g.ny;
+    d.nz = g.nz;
+    d.steps = g.steps;
+    d.px = px;
+    d.segs = segs;
+    d.pc = pc;
+    d.grid_id = i;
+    for (int j = 0; j < 7; ++j) d.k[j] = g.coeff[j];
+    d.k[7] = -0.0f;
+    const std::pair<int, int> key(cl, v);
+    int ci = -1;
+    for (size_t j = 0; j < keys.size(); ++j)
+      if (keys[j] == key) ci = (int)j;
+    if (ci < 0) {
+      ci = (int)keys.size();
+      keys.push_back(key);
+      b->rclasses.emplace_back();
+      b->rclasses.back().cluster = cl;
+      b->rclasses.back().variant = v;
+    }
+    ResidentClass& rc = b->rclasses[ci];
+    rc.grids.push_back(i);
+    rc.smem = std::max(rc.smem, (size_t)((pc + 1) * plane * 4));
+    b->rclass_of[i] = ci;
+    b->resident_ok[i] = 1;
+  }
+  // Classes the GPU cannot schedule (no cluster of that size and shared
+  // memory fits) hand their grids back to the per-step kinds.
+  for (size_t ci = 0; ci < b->rclasses.size(); ++ci) {
+    ResidentClass& rc = b->rclasses[ci];
+    int maxc = 0;
+    if (d3d::resident_max_clusters(rc.variant, rc.cluster, rc.smem,
+                                   &maxc) != cudaSuccess) {
+      cudaGetLastError();
+      maxc = 0;
+    }
+    rc.nclusters = std::min<int>(maxc, (int)rc.grids.size());
+    if (rc.nclusters < 1)
+      for (int id : rc.grids) b->resident_ok[id] = 0;
+  }
+  std::vector<ResidentClass> kept;
+  for (ResidentClass& rc : b->rclasses)
+    if (rc.nclusters >= 1) kept.push_back(std::move(rc));
+  b->rclasses = std::move(kept);
+  for (size_t ci = 0; ci < b->rclasses.size(); ++ci) {
+    ResidentClass& rc = b->rclasses[ci];
+    // Largest work first: the last grids to start are the shortest.
+    std::stable_sort(rc.grids.begin(), rc.grids.end(), [&](int x, int y) {
+      const d3d_batch_grid &gx = b->grids[x], &gy = b->grids[y];
+      return (double)gx.nx * gx.ny * gx.nz * gx.steps >
+             (double)gy.nx * gy.ny * gy.nz * gy.steps;
+    });
+    std::vector<d3d::ResidentDesc> descs;
+    for (int id : rc.grids) {
+      descs.push_back(b->rdesc[id]);
+      b->rclass_of[id] = (int)ci;
+    }
+    int r = upload(descs, &rc.d_descs, "resident descriptors");
+    if (r) return r;
+    B_TRY(cudaMalloc(&rc.d_queue, sizeof(unsigned)),
+          "cudaMalloc (resident work counter)");
+  }
+  return D3D_OK;
+}
+
+void free_resident(d3d_batch b) {
+  for (ResidentClass& rc : b->rclasses) {
+    if (rc.d_descs) cudaFree(rc.d_descs);
+    if (rc.d_queue) cudaFree(rc.d_queue);
+    rc.d_descs = nullptr;
+    rc.d_queue = nullptr;
+  }
+}
+
+// Puts every grid (steps >= 0) into its size class, leaving out the grids
+// the cluster-resident kernel runs when it is on, and rebuilds the classes'
+// work lists and the repitch lists.
+int assign_grids(d3d_batch b) {
+  for (ClassPlan& c : b->cls) {
+    c.grids.clear();
+    c.max_steps = 0;
+  }
+  b->max_steps = 0;
+  std::vector<int2> classic;
+  for (int i = 0; i < (int)b->grids.size(); ++i) {
+    if (b->resident_on && b->resident_ok[i]) continue;
+    ClassPlan& c = b->cls[class_of(b->grids[i].nx)];
+    c.grids.push_back(i);
+    c.max_steps = std::max(c.max_steps, b->grids[i].steps);
+    b->max_steps = std::max(b->max_steps, b->grids[i].steps);
+    classic.push_back(make_int2(i, b->grids[i].steps));
+  }
+  b->total_items = 0;
+  for (ClassPlan& c : b->cls) {
+    std::stable_sort(c.grids.begin(), c.grids.end(), [&](int x, int y) {
+      return b->grids[x].steps > b->grids[y].steps;
+    });
+    int rc = build_class(b, c);
+    if (rc) return rc;
+    for (int a : c.active) b->total_items += a;
+  }
+  if (b->d_classic_steps) cudaFree(b->d_classic_steps);
+  b->d_classic_steps = nullptr;
+  b->n_classic = (int)classic.size();
+  int rc = upload(classic, &b->d_classic_steps, "batch step counts");
+  if (rc) return rc;
+  return build_repitch(b);
+}
+
+// A whole run on stream s: the cluster-resident launches on side streams
+// forked from s, the per-step launches of the other grids on s meanwhile,
+// then s waits for the side streams.  Every grid's step counter is zeroed
+// first; the resident kernel advances its grids' counters step by step,
+// and one small launch after the per-step path sets the other grids'.
+int enqueue_all(d3d_batch b, cudaStream_t s, unsigned long long* launches) {
+  unsigned long long n = 0;
+  B_TRY(cudaMemsetAsync(b->d_counters, 0, b->grids.size() * sizeof(int), s),
+        "counter reset");
+  bool used[kSideStreams] = {};
+  if (b->resident_on && !b->rclasses.empty()) {
+    B_TRY(cudaEventRecord(b->fork, s), "cudaEventRecord (fork)");
+    for (size_t ci = 0; ci < b->rclasses.size(); ++ci) {
+      const ResidentClass& rc = b->rclasses[ci];
+      const int k = (int)(ci % kSideStreams);
+      if (!used[k]) {
+        B_TRY(cudaStreamWaitEvent(b->side[k], b->fork, 0),
+              "cudaStreamWaitEvent (fork)");
+        used[k] = true;
+      }
+      B_TRY(cudaMemsetAsync(rc.d_queue, 0, sizeof(unsigned), b->side[k]),
+            "work counter reset");
+      B_TRY(d3d::launch_resident(rc.variant, rc.d_descs,
+                                 (int)rc.grids.size(), rc.d_queue,
+                                 b->d_counters, rc.cluster, rc.nclusters,
+                                 rc.smem, b->side[k]),
+            "resident launch");
+      ++n;
+    }
+  }
+  if (b->n_rep) {
+    B_TRY(d3d::launch_repitch_multi(b->d_rep_in, b->n_rep, true, s),
+          "repitch launch");
+    ++n;
+  }
+  unsigned long long steps_launched = 0;
+  int rc = enqueue_run(b, s, -1, b->max_steps, &steps_launched);
+  if (rc) return rc;
+  n += steps_launched;
+  if (b->n_rep) {
+    B_TRY(d3d::launch_repitch_multi(b->d_rep_out, b->n_rep, false, s),
+          "repitch launch");
+    ++n;
+  }
+  if (b->n_classic) {
+    B_TRY(d3d::launch_set_counters(b->d_classic_steps, b->n_classic,
+                                   b->d_counters, s),
+          "counter launch");
+    ++n;
+  }
+  for (int k = 0; k < kSideStreams; ++k) {
+    if (!used[k]) continue;
+    B_TRY(cudaEventRecord(b->join[k], b->side[k]), "cudaEventRecord (join)");
+    B_TRY(cudaStreamWaitEvent(s, b->join[k], 0), "cudaStreamWaitEvent");
+  }
+  if (launches) *launches = n;
+  return D3D_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -493,33 +729,28 @@ int d3d_batch_create(const d3d_batch_grid* grids, int n, void* arena,
     cudaGetLastError();
     b->pitched = nullptr;
   }
-  for (int i = 0; i < n; ++i) {
-    ClassPlan& c = b->cls[class_of(grids[i].nx)];
-    c.grids.push_back(i);
-    c.max_steps = std::max(c.max_steps, grids[i].steps);
-    b->max_steps = std::max(b->max_steps, grids[i].steps);
-  }
-  for (auto& c : b->cls) {
-    std::stable_sort(c.grids.begin(), c.grids.end(), [&](int x, int y) {
-      return b->grids[x].steps > b->grids[y].steps;
-    });
-    c.kind = b->pitched ? kDefaultKind : 0;
-    int rc = build_class(b, c);
-    if (rc) {
-      d3d_batch_destroy(b);
-      return rc;
-    }
-    for (int a : c.active) b->total_items += a;
-  }
-  int rc = build_repitch(b);
+  for (auto& c : b->cls) c.kind = b->pitched ? kDefaultKind : 0;
+  int rc = plan_resident(b);
+  if (!rc) rc = assign_grids(b);
   if (rc) {
     d3d_batch_destroy(b);
     return rc;
   }
-  if (cudaEventCreate(&b->ev[0]) != cudaSuccess ||
-      cudaEventCreate(&b->ev[1]) != cudaSuccess) {
+  bool ok = cudaMalloc(&b->d_counters, n * sizeof(int)) == cudaSuccess &&
+            cudaMemset(b->d_counters, 0, n * sizeof(int)) == cudaSuccess &&
+            cudaEventCreate(&b->ev[0]) == cudaSuccess &&
+            cudaEventCreate(&b->ev[1]) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) ==
+                cudaSuccess;
+  for (int k = 0; ok && k < kSideStreams; ++k)
+    ok = cudaStreamCreateWithFlags(&b->side[k], cudaStreamNonBlocking) ==
+             cudaSuccess &&
+         cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming) ==
+             cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
     d3d_batch_destroy(b);
-    return bfail(D3D_E_CUDA, "cudaEventCreate");
+    return bfail(D3D_E_CUDA, "batch streams, events or step counters");
   }
   *out = b;
   return D3D_OK;
@@ -529,6 +760,10 @@ int d3d_batch_autotune(d3d_batch b, void* stream) {
   if (!b) return bfail(D3D_E_INVALID, "NULL batch");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   drop_graph(b);
+  // Per-class kinds are tuned with every grid in its class.
+  b->resident_on = false;
+  int arc = assign_grids(b);
+  if (arc) return arc;
   b->total_items = 0;
   for (int ci = 0; ci < kNumClasses; ++ci) {
     ClassPlan& c = b->cls[ci];
@@ -563,30 +798,55 @@ int d3d_batch_autotune(d3d_batch b, void* stream) {
   }
   for (const ClassPlan& c : b->cls)
     for (int a : c.active) b->total_items += a;
-  return build_repitch(b);
+  int rc = build_repitch(b);
+  if (rc) return rc;
+  // Then the whole run with and without the cluster-resident kernel for
+  // the grids it fits (the others keep the kinds just picked).
+  bool any = false;
+  for (char ok : b->resident_ok) any = any || ok;
+  if (!any) return D3D_OK;
+  float ms[2] = {0.0f, 0.0f};
+  for (int on = 0; on < 2; ++on) {
+    b->resident_on = on != 0;
+    rc = assign_grids(b);
+    if (rc) return rc;
+    rc = enqueue_all(b, s, nullptr);  // warm-up
+    if (rc) return rc;
+    B_TRY(cudaEventRecord(b->ev[0], s), "cudaEventRecord");
+    rc = enqueue_all(b, s, nullptr);
+    if (rc) return rc;
+    B_TRY(cudaEventRecord(b->ev[1], s), "cudaEventRecord");
+    B_TRY(cudaEventSynchronize(b->ev[1]), "cudaEventSynchronize");
+    B_TRY(cudaEventElapsedTime(&ms[on], b->ev[0], b->ev[1]), "elapsed");
+  }
+  b->resident_on = ms[1] < ms[0];
+  return assign_grids(b);
 }
 
 int d3d_batch_set_kind(d3d_batch b, int kind) {
   if (!b) return bfail(D3D_E_INVALID, "NULL batch");
   if (kind < 0 || kind >= kNumKinds)
     return bfail(D3D_E_INVALID, "no such kernel kind");
+  if (kind == kResidentKind) {
+    // Every grid the cluster-resident kernel fits runs on it; the others
+    // take the strip kind (the march kind without pitched copies).
+    drop_graph(b);
+    b->resident_on = true;
+    for (ClassPlan& c : b->cls) c.kind = b->pitched ? kDefaultKind : 0;
+    return assign_grids(b);
+  }
   if (kind_nr(kind) && !b->pitched)
     return bfail(D3D_E_UNSUPPORTED,
                  "no device memory was left for the pitched copies");
   if (kind_two(kind))
-    for (const ClassPlan& c : b->cls)
-      if (!class_takes_two_step(b, c))
+    for (int i = 0; i < (int)b->grids.size(); ++i)
+      if (pitch_of(b->grids[i].nx) > d3d::kStripMaxW)
         return bfail(D3D_E_UNSUPPORTED,
                      "two-step kinds need grids at most 248 floats wide");
   drop_graph(b);
-  b->total_items = 0;
-  for (ClassPlan& c : b->cls) {
-    c.kind = kind;
-    int rc = build_class(b, c);
-    if (rc) return rc;
-    for (int a : c.active) b->total_items += a;
-  }
-  return build_repitch(b);
+  b->resident_on = false;
+  for (ClassPlan& c : b->cls) c.kind = kind;
+  return assign_grids(b);
 }
 
 int d3d_batch_run(d3d_batch b, void* stream, float* kernel_ms) {
@@ -603,21 +863,13 @@ int d3d_batch_run(d3d_batch b, void* stream, float* kernel_ms) {
     B_TRY(cudaStreamBeginCapture(b->capture_stream,
                                  cudaStreamCaptureModeThreadLocal),
           "cudaStreamBeginCapture");
-    // Strip-kind grids: inputs into the pitched copies, the steps, results
-    // back into the caller's arena.
-    unsigned long long steps_launched = 0;
-    cudaError_t e = d3d::launch_repitch_multi(b->d_rep_in, b->n_rep, true,
-                                              b->capture_stream);
-    int rc = e == cudaSuccess ? enqueue_run(b, b->capture_stream, -1,
-                                            b->max_steps, &steps_launched)
-                              : bcuda(e, "repitch launch");
-    if (!rc) {
-      e = d3d::launch_repitch_multi(b->d_rep_out, b->n_rep, false,
-                                    b->capture_stream);
-      if (e != cudaSuccess) rc = bcuda(e, "repitch launch");
-    }
+    // The cluster-resident launches (forked), strip-kind grids' inputs
+    // into the pitched copies, the per-step launches, results back into
+    // the caller's arena, the step counters; then the join.
+    unsigned long long launched = 0;
+    int rc = enqueue_all(b, b->capture_stream, &launched);
     cudaGraph_t g = nullptr;
-    e = cudaStreamEndCapture(b->capture_stream, &g);
+    cudaError_t e = cudaStreamEndCapture(b->capture_stream, &g);
     if (rc) {
       if (g) cudaGraphDestroy(g);
       return rc;
@@ -629,7 +881,7 @@ int d3d_batch_run(d3d_batch b, void* stream, float* kernel_ms) {
       b->exec = nullptr;
       return bcuda(e, "cudaGraphInstantiate");
     }
-    b->launches_per_run = steps_launched + (b->n_rep ? 2 : 0);
+    b->launches_per_run = launched;
   }
   B_TRY(cudaEventRecord(b->ev[0], s), "cudaEventRecord");
   B_TRY(cudaGraphLaunch(b->exec, s), "cudaGraphLaunch");
@@ -644,11 +896,28 @@ int d3d_batch_run(d3d_batch b, void* stream, float* kernel_ms) {
 
 int d3d_batch_info(d3d_batch b, char* buf, size_t len) {
   if (!b || !buf) return bfail(D3D_E_INVALID, "NULL argument");
+  int nres = 0;
+  if (b->resident_on)
+    for (const ResidentClass& rc : b->rclasses) nres += (int)rc.grids.size();
   int used = snprintf(buf, len,
                       "{\"grids\": %zu, \"max_steps\": %d, \"items\": %lld, "
-                      "\"launches_per_run\": %llu, \"classes\": [",
+                      "\"launches_per_run\": %llu, \"resident\": "
+                      "{\"on\": %s, \"grids\": %d, \"classes\": [",
                       b->grids.size(), b->max_steps, b->total_items,
-                      b->launches_per_run);
+                      b->launches_per_run,
+                      b->resident_on ? "true" : "false", nres);
+  for (size_t ci = 0; b->resident_on && ci < b->rclasses.size() &&
+                      used < (int)len; ++ci) {
+    const ResidentClass& rc = b->rclasses[ci];
+    used += snprintf(buf + used, len - used,
+                     "%s{\"cluster\": %d, \"threads\": %d, \"grids\": "
+                     "%zu, \"clusters\": %d, \"smem\": %zu}",
+                     ci ? ", " : "", rc.cluster,
+                     d3d::resident_variant(rc.variant).threads,
+                     rc.grids.size(), rc.nclusters, rc.smem);
+  }
+  if (used < (int)len)
+    used += snprintf(buf + used, len - used, "]}, \"classes\": [");
   for (int ci = 0; ci < kNumClasses && used < (int)len; ++ci) {
     const ClassPlan& c = b->cls[ci];
     const int nr = kind_nr(c.kind);
@@ -669,9 +938,27 @@ int d3d_batch_info(d3d_batch b, char* buf, size_t len) {
   return D3D_OK;
 }
 
+int d3d_batch_progress(d3d_batch b, int* steps_done, int n) {
+  if (!b || !steps_done) return bfail(D3D_E_INVALID, "NULL argument");
+  if (n != (int)b->grids.size())
+    return bfail(D3D_E_INVALID, "n must be the batch's grid count");
+  B_TRY(cudaMemcpy(steps_done, b->d_counters, (size_t)n * sizeof(int),
+                   cudaMemcpyDeviceToHost),
+        "D2H step counters");
+  return D3D_OK;
+}
+
 int d3d_batch_destroy(d3d_batch b) {
   if (!b) return D3D_OK;
   drop_graph(b);
+  free_resident(b);
+  if (b->d_counters) cudaFree(b->d_counters);
+  if (b->d_classic_steps) cudaFree(b->d_classic_steps);
+  for (int k = 0; k < kSideStreams; ++k) {
+    if (b->side[k]) cudaStreamDestroy(b->side[k]);
+    if (b->join[k]) cudaEventDestroy(b->join[k]);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
   for (auto& c : b->cls) free_class(c);
   if (b->d_rep_in) cudaFree(b->d_rep_in);
   if (b->d_rep_out) cudaFree(b->d_rep_out);

@@ -54,12 +54,14 @@ cudaError_t encode_field_map(CUtensorMap* map, const void* ptr, int nx, int ny,
 cudaError_t launch_scale_copy(const float* in, float* out, size_t n, float cc,
                               cudaStream_t s);
 
-// One time step, f2 = stencil(f1), with the TMA-staged z-march.
+// One time step, f2 = stencil(f1), with the TMA-staged z-march.  Only
+// output planes [zb, ze) are written (ze < 0: nz); the boundary clamps
+// stay at the field's own ends.
 cudaError_t launch_step_tma(const CUtensorMap& src, void* f2, int nx, int ny,
                             int nz, const void* coef, int dtype, int variant,
                             int zchunk_override, int flip_y,
                             cudaStream_t stream, unsigned* dev_err,
-                            LaunchInfo* info);
+                            LaunchInfo* info, int zb = 0, int ze = -1);
 int tma_box_x(int dtype);
 int tma_box_y(int variant);
 
@@ -67,7 +69,7 @@ int tma_box_y(int variant);
 cudaError_t launch_step_generic(const void* f1, void* f2, int nx, int ny,
                                 int nz, const void* coef, int dtype,
                                 int flip_y, cudaStream_t stream,
-                                LaunchInfo* info);
+                                LaunchInfo* info, int zb = 0, int ze = -1);
 
 // One 2D 5-point time step (diffusion::Diffusion with nd = 2), any shape
 // and alignment; ychunk_override = rows per warp task (0 = automatic).
@@ -209,6 +211,47 @@ cudaError_t launch_repitch_multi(const RepitchDesc* d, int n,
 // src and dst must not overlap.
 cudaError_t launch_repitch(const float* src, float* dst, int nx, int px,
                            long long rows, bool to_pitched, cudaStream_t s);
+
+// One grid of the cluster-resident multi-grid kernel (d3d_resident.cu):
+// dense fields in and out (out may equal in), the pitch px = ceil4(nx) and
+// segs = px / 4 of its shared-memory rows, pc planes per CTA of its
+// cluster, and the index of its step counter.
+struct ResidentDesc {
+  const float* in;
+  float* out;
+  int nx, ny, nz, steps;
+  int px, segs, pc, grid_id;
+  float k[8];  // ce, cw, cn, cs, ct, cb, cc, and -0.0
+};
+// Thread shapes: `threads` a CTA, at most `units` 16-byte row segments of
+// a plane a thread (a plane of segs * ny segments fits when
+// segs * ny <= threads * units).
+struct ResidentVariant {
+  int threads, units;
+};
+constexpr int kNumResidentVariants = 5;
+constexpr int kResidentMaxCluster = 16;
+// Dynamic shared memory a CTA may hold: its pc planes and a halo plane.
+constexpr size_t kResidentSmemMax = 232448 - 1024;
+const ResidentVariant& resident_variant(int v);
+// Opts the kernels into the full shared memory and 16-CTA clusters on the
+// current device (once per device).
+cudaError_t resident_prepare();
+// Clusters of `cluster` CTAs with `smem` bytes each that fit on the GPU at
+// once (0: not schedulable).
+cudaError_t resident_max_clusters(int variant, int cluster, size_t smem,
+                                  int* out);
+// A persistent launch of `nclusters` clusters walking descs[0, ngrids)
+// through the work counter *queue (zero it before the launch).
+cudaError_t launch_resident(int variant, const ResidentDesc* descs,
+                            int ngrids, unsigned* queue, int* steps_done,
+                            int cluster, int nclusters, size_t smem,
+                            cudaStream_t s);
+
+// counters[id_steps[i].x] = id_steps[i].y for i < n: the step counters
+// of grids that ran on the per-step path, set after its last launch.
+cudaError_t launch_set_counters(const int2* id_steps, int n, int* counters,
+                                cudaStream_t s);
 
 // This device's kernel error word (bounded-wait failures).
 unsigned* device_error_word();

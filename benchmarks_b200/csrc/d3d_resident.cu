@@ -1,0 +1,379 @@
+// Cluster-resident multi-grid kernel: whole small grids live in shared
+// memory for all of their steps.
+//
+// A batch of small grids (the 16..96-per-axis batch: at most 3.5 MiB per
+// buffer) streams every grid through HBM once per step when each step is a
+// launch: 8 bytes per point-update, whatever the kernel.  Here a thread-
+// block cluster of C CTAs (C <= 16) holds one grid in its shared memory,
+// split into z slabs of `pc` planes per CTA, and runs all of that grid's
+// steps before it takes the next grid: HBM sees the grid once on the way in
+// and once on the way out.  The launch is persistent: one launch per
+// (cluster size, thread shape) class walks that class's grids, largest work
+// first, through an atomic work counter, and records each grid's completed
+// steps in a per-grid counter.
+//
+// One step (the reference's update, diffusion3d_openmp.cc:43-71, evaluated
+// with d3d::point_seg: same order, same rounding):
+//   1. cluster barrier: the previous step's planes (or the loaded input)
+//      are complete in every CTA;
+//   2. each thread pulls, for its own columns, the plane below its slab
+//      (the b of its first plane) from the lower neighbour CTA's shared
+//      memory into registers, and the plane above its slab (the t of its
+//      last plane) into a one-plane halo buffer of its own CTA (DSMEM loads,
+//      ld.shared::cluster; no TMA, no multicast);
+//   3. cluster barrier: every pull is done, so planes may be overwritten;
+//   4. z-march over the slab, in place: b and c of each thread's 16-byte
+//      segments ride in registers, t, n, s come from shared memory, x
+//      neighbours from shuffles (lanes at a row or warp edge read the
+//      staged word); a block barrier separates the reads of plane p from
+//      the writes of its new values.
+// Replicated boundaries: x = 0 and the last segment take their own value
+// (the pads x in [nx, px) hold copies of column nx-1 and are rewritten each
+// step), y = 0 / ny-1 read their own row, z = 0 / nz-1 their own plane.
+//
+// Synchronisation is the hardware cluster barrier only (every CTA of a
+// cluster runs the same loop bounds, read from the same descriptor); no
+// thread spins on a flag, so there is no wait to bound.  A CTA with no
+// planes (nz < C * pc) still takes part in every barrier.
+#include <algorithm>
+#include <cstdio>
+
+#include "d3d_common.cuh"
+#include "d3d_kernels.h"
+
+namespace d3d {
+
+namespace {
+
+// Every thread of every CTA of the cluster arrives (release) and waits
+// (acquire): shared-memory writes before it, local or remote, are visible
+// to every thread of the cluster after it.  The non-.aligned forms, so a
+// warp need not be converged when it reaches the barrier.
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile(
+      "barrier.cluster.arrive.release;\n\t"
+      "barrier.cluster.wait.acquire;" ::
+          : "memory");
+}
+
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+__device__ __forceinline__ unsigned cluster_size() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+
+// The shared::cluster address of `cta_addr` (a shared::cta address) in CTA
+// `rank` of this cluster.
+__device__ __forceinline__ uint32_t map_to_rank(uint32_t cta_addr,
+                                                unsigned rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;"
+               : "=r"(r)
+               : "r"(cta_addr), "r"(rank));
+  return r;
+}
+
+__device__ __forceinline__ V16<float> ld16_cluster(uint32_t addr) {
+  V16<float> v;
+  asm volatile("ld.shared::cluster.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.e[0]), "=f"(v.e[1]), "=f"(v.e[2]), "=f"(v.e[3])
+               : "r"(addr)
+               : "memory");
+  return v;
+}
+
+__device__ __forceinline__ int ld_cluster_s32(uint32_t addr) {
+  int v;
+  asm volatile("ld.shared::cluster.s32 %0, [%1];"
+               : "=r"(v)
+               : "r"(addr)
+               : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st16_shared(float* p, const V16<float>& v) {
+  *reinterpret_cast<int4*>(p) = *reinterpret_cast<const int4*>(&v);
+}
+
+// Flag bits of a thread's unit (one 16-byte segment of one row).
+enum : unsigned {
+  kValid = 1u,
+  kWOwn = 2u,    // x = 0: w is the centre value
+  kWSm = 4u,     // lane 0 inside a row: w is the staged word before
+  kEOwn = 8u,    // last segment of the row: e is the centre value
+  kESm = 16u,    // lane 31 inside a row: e is the staged word after
+  kNOwn = 32u,   // y = 0: n is the own row
+  kSOwn = 64u,   // y = ny-1: s is the own row
+  kCross = 128u  // the segment holds x = nx-1 followed by pads
+};
+
+template <int NT, int UMAX>
+__device__ __forceinline__ void resident_grid(const ResidentDesc& d,
+                                              unsigned rank, float* sm,
+                                              int* __restrict__ steps_done,
+                                              int g) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int nx = d.nx, ny = d.ny, nz = d.nz, px = d.px, S = d.segs;
+  const int pc = d.pc;
+  const int plane = px * ny;
+  const int z0 = (int)rank * pc;
+  const int z1 = min(nz, z0 + pc);
+  const int np = max(0, z1 - z0);
+  float* halo = sm + pc * plane;  // the plane above the slab (t of z1-1)
+
+  // Load the slab: rows of nx floats into rows of px, pads from nx-1.
+  {
+    const float* __restrict__ src = d.in + (size_t)z0 * ny * nx;
+    const int rows = np * ny;
+    for (int r = tid >> 5; r < rows; r += NT / 32) {
+      const float* in = src + (size_t)r * nx;
+      float* o = sm + r * px;
+      for (int x = lane; x < px; x += 32) o[x] = in[min(x, nx - 1)];
+    }
+  }
+
+  // This thread's units u = tid + i * NT of the plane (S segments a row).
+  const int units = S * ny;
+  int c_off[UMAX];
+  unsigned fl[UMAX];  // flag bits; bits 8..9: index of x = nx-1 if kCross
+#pragma unroll
+  for (int i = 0; i < UMAX; ++i) {
+    const int u = tid + i * NT;
+    const bool valid = u < units;
+    const int uu = valid ? u : 0;
+    const int y = uu / S, seg = uu - y * S;
+    const int xg = 4 * seg;
+    c_off[i] = y * px + xg;
+    unsigned f = valid ? kValid : 0u;
+    if (seg == 0) f |= kWOwn;
+    else if (lane == 0) f |= kWSm;
+    if (seg == S - 1) f |= kEOwn;
+    else if (lane == 31) f |= kESm;
+    if (y == 0) f |= kNOwn;
+    if (y == ny - 1) f |= kSOwn;
+    if (xg + 4 > nx) f |= kCross | ((unsigned)(nx - 1 - xg) << 8);
+    fl[i] = f;
+  }
+  const Coef<float> k{d.k[0], d.k[1], d.k[2], d.k[3],
+                      d.k[4], d.k[5], d.k[6], d.k[7]};
+  const Coef2 kk = coef2(k);
+  const uint32_t sm_base = smem_u32(sm);
+  const uint32_t below =
+      z0 > 0 ? map_to_rank(sm_base, rank - 1) + 4u * (pc - 1) * plane : 0u;
+  const uint32_t above = z1 < nz ? map_to_rank(sm_base, rank + 1) : 0u;
+
+  V16<float> bq[UMAX], cq[UMAX], nv[UMAX];
+  for (int s = 0; s < d.steps; ++s) {
+    cluster_sync_all();  // planes of the previous step complete everywhere
+    if (np > 0) {
+#pragma unroll
+      for (int i = 0; i < UMAX; ++i) {
+        bq[i] = z0 > 0 ? ld16_cluster(below + 4u * c_off[i])
+                       : ld16_shared(sm + c_off[i]);
+        if (z1 < nz && (fl[i] & kValid))
+          st16_shared(halo + c_off[i], ld16_cluster(above + 4u * c_off[i]));
+      }
+    }
+    cluster_sync_all();  // every pull done: planes may be overwritten
+    if (np > 0) {
+#pragma unroll
+      for (int i = 0; i < UMAX; ++i) cq[i] = ld16_shared(sm + c_off[i]);
+      for (int p = 0; p < np; ++p) {
+        float* pl = sm + p * plane;
+        const float* tp =
+            p + 1 < np ? pl + plane : (z1 < nz ? halo : pl);
+#pragma unroll
+        for (int i = 0; i < UMAX; ++i) {
+          const unsigned f = fl[i];
+          const V16<float> c = cq[i];
+          const V16<float> t = ld16_shared(tp + c_off[i]);
+          const V16<float> n =
+              ld16_shared(pl + c_off[i] - ((f & kNOwn) ? 0 : px));
+          const V16<float> so =
+              ld16_shared(pl + c_off[i] + ((f & kSOwn) ? 0 : px));
+          float wl = __shfl_up_sync(0xffffffffu, c.e[3], 1);
+          float er = __shfl_down_sync(0xffffffffu, c.e[0], 1);
+          wl = ld_shared_if(f & kWSm, pl + c_off[i] - 1, wl);
+          if (f & kWOwn) wl = c.e[0];
+          er = ld_shared_if(f & kESm, pl + c_off[i] + 4, er);
+          if (f & kEOwn) er = c.e[3];
+          V16<float> o = point_seg<float>(kk, c, n, so, bq[i], t, wl, er);
+          if (f & kCross) {
+            const unsigned jh = (f >> 8) & 3u;
+            if (jh < 1) o.e[1] = o.e[0];
+            if (jh < 2) o.e[2] = o.e[1];
+            o.e[3] = o.e[2];
+          }
+          nv[i] = o;
+          bq[i] = c;
+          cq[i] = t;
+        }
+        __syncthreads();  // plane p read everywhere: overwrite it
+#pragma unroll
+        for (int i = 0; i < UMAX; ++i)
+          if (fl[i] & kValid) st16_shared(pl + c_off[i], nv[i]);
+      }
+    }
+    if (rank == 0 && tid == 0)
+      *reinterpret_cast<volatile int*>(steps_done + g) = s + 1;
+  }
+  __syncthreads();
+  // Store the slab: the first nx floats of each row.
+  {
+    float* __restrict__ dst = d.out + (size_t)z0 * ny * nx;
+    const int rows = np * ny;
+    for (int r = tid >> 5; r < rows; r += NT / 32) {
+      float* o = dst + (size_t)r * nx;
+      const float* in = sm + r * px;
+      for (int x = lane; x < nx; x += 32) o[x] = in[x];
+    }
+  }
+}
+
+template <int NT, int UMAX>
+__global__ void __launch_bounds__(NT)
+    resident_kernel(const ResidentDesc* __restrict__ descs, int ngrids,
+                    unsigned* __restrict__ queue,
+                    int* __restrict__ steps_done) {
+  extern __shared__ __align__(16) float sm[];
+  __shared__ int next_grid;
+  const unsigned rank = cluster_rank();
+  for (;;) {
+    if (rank == 0 && threadIdx.x == 0)
+      next_grid = (int)atomicAdd(queue, 1u);
+    cluster_sync_all();
+    const int g = rank == 0 ? next_grid
+                            : ld_cluster_s32(map_to_rank(
+                                  smem_u32(&next_grid), 0));
+    cluster_sync_all();  // everyone has read it before rank 0 rewrites it
+    if (g >= ngrids) break;
+    resident_grid<NT, UMAX>(descs[g], rank, sm, steps_done,
+                            descs[g].grid_id);
+  }
+}
+
+// (threads, units a thread at most): a plane of S * ny 16-byte segments
+// fits variant v when S * ny <= threads * units.
+const ResidentVariant kResident[kNumResidentVariants] = {
+    {128, 2}, {256, 2}, {512, 2}, {512, 4}, {384, 6}};
+
+template <int NT, int UMAX>
+cudaError_t launch_v(const ResidentDesc* descs, int ngrids, unsigned* queue,
+                     int* steps_done, int cluster, int nclusters,
+                     size_t smem, cudaStream_t s) {
+  auto kern = resident_kernel<NT, UMAX>;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(nclusters * cluster));
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, descs, ngrids, queue, steps_done);
+}
+
+template <int NT, int UMAX>
+cudaError_t prepare_v() {
+  auto kern = resident_kernel<NT, UMAX>;
+  cudaError_t e = cudaFuncSetAttribute(
+      kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      (int)kResidentSmemMax);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(
+      kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+
+template <int NT, int UMAX>
+cudaError_t max_clusters_v(int cluster, size_t smem, int* out) {
+  auto kern = resident_kernel<NT, UMAX>;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)cluster);
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaOccupancyMaxActiveClusters(out, kern, &cfg);
+}
+
+__global__ void set_counters_kernel(const int2* __restrict__ id_steps, int n,
+                                    int* __restrict__ counters) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x)
+    counters[id_steps[i].x] = id_steps[i].y;
+}
+
+}  // namespace
+
+const ResidentVariant& resident_variant(int v) { return kResident[v]; }
+
+cudaError_t launch_set_counters(const int2* id_steps, int n, int* counters,
+                                cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int blocks = std::min((n + 255) / 256, 148);
+  set_counters_kernel<<<blocks, 256, 0, s>>>(id_steps, n, counters);
+  return cudaGetLastError();
+}
+
+cudaError_t resident_prepare() {
+  static int done_dev = -1;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (done_dev == dev) return cudaSuccess;
+  if ((e = prepare_v<128, 2>()) != cudaSuccess) return e;
+  if ((e = prepare_v<256, 2>()) != cudaSuccess) return e;
+  if ((e = prepare_v<512, 2>()) != cudaSuccess) return e;
+  if ((e = prepare_v<512, 4>()) != cudaSuccess) return e;
+  if ((e = prepare_v<384, 6>()) != cudaSuccess) return e;
+  done_dev = dev;
+  return cudaSuccess;
+}
+
+cudaError_t resident_max_clusters(int variant, int cluster, size_t smem,
+                                  int* out) {
+  *out = 0;
+  switch (variant) {
+    case 0: return max_clusters_v<128, 2>(cluster, smem, out);
+    case 1: return max_clusters_v<256, 2>(cluster, smem, out);
+    case 2: return max_clusters_v<512, 2>(cluster, smem, out);
+    case 3: return max_clusters_v<512, 4>(cluster, smem, out);
+    case 4: return max_clusters_v<384, 6>(cluster, smem, out);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_resident(int variant, const ResidentDesc* descs,
+                            int ngrids, unsigned* queue, int* steps_done,
+                            int cluster, int nclusters, size_t smem,
+                            cudaStream_t s) {
+  if (ngrids <= 0 || nclusters <= 0) return cudaSuccess;
+  if (cluster < 1 || cluster > kResidentMaxCluster ||
+      smem > kResidentSmemMax)
+    return cudaErrorInvalidValue;
+  switch (variant) {
+    case 0: return launch_v<128, 2>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case 1: return launch_v<256, 2>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case 2: return launch_v<512, 2>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case 3: return launch_v<512, 4>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case 4: return launch_v<384, 6>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace d3d

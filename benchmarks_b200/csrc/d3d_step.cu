@@ -57,7 +57,8 @@ template <typename T, int BY, int S, bool FLIP>
 __global__ void __launch_bounds__(StepTmaCfg<T, BY, S>::THREADS)
     step_tma_kernel(const __grid_constant__ CUtensorMap src,
                     T* __restrict__ dst, int nx, int ny, int nz, Coef<T> k,
-                    int zchunk, unsigned* __restrict__ dev_err) {
+                    int zchunk, int zb, int ze,
+                    unsigned* __restrict__ dev_err) {
   using C = StepTmaCfg<T, BY, S>;
   constexpr int V = C::V;
   constexpr int RPW = C::RPW;
@@ -71,8 +72,10 @@ __global__ void __launch_bounds__(StepTmaCfg<T, BY, S>::THREADS)
   const int warp = threadIdx.x >> 5;
   const int x0 = blockIdx.x * C::BX;
   const int y0 = blockIdx.y * BY;
-  const int z0 = blockIdx.z * zchunk;
-  const int z1 = min(nz, z0 + zchunk);
+  // Output planes [zb, ze) of the field, zchunk a CTA (the clamps below
+  // use the field's own ends, 0 and nz - 1).
+  const int z0 = zb + blockIdx.z * zchunk;
+  const int z1 = min(ze, z0 + zchunk);
   if (z0 >= z1) return;
   const int pbase = z0 > 0 ? z0 - 1 : 0;  // first plane loaded (b of z0)
   const int plast = min(z1, nz - 1);      // last plane needed (t of z1-1)
@@ -236,10 +239,11 @@ template <> struct GenTile<double> { static constexpr int BX = 32, BY = 8; };
 template <typename T, bool FLIP>
 __global__ void __launch_bounds__(256)
     step_generic_kernel(const T* __restrict__ src, T* __restrict__ dst,
-                        int nx, int ny, int nz, Coef<T> k, int zchunk) {
+                        int nx, int ny, int nz, Coef<T> k, int zchunk,
+                        int zb, int ze) {
   constexpr int BX = GenTile<T>::BX, BY = GenTile<T>::BY;
-  const int z0 = blockIdx.z * zchunk;
-  const int z1 = min(nz, z0 + zchunk);
+  const int z0 = zb + blockIdx.z * zchunk;
+  const int z1 = min(ze, z0 + zchunk);
   if (z0 >= z1) return;
   if constexpr (sizeof(T) == 4) {
     __shared__ __align__(16) float stage[2][MarchTile2<BX, BY>::E];
@@ -326,6 +330,7 @@ int pick_zchunk(int nz, long tiles, int ctas_per_sm, int min_chunk) {
 template <typename T, int BY, int S, bool FLIP>
 cudaError_t launch_tma_t(const CUtensorMap& src, void* f2, int nx, int ny,
                          int nz, const void* coef, int zchunk_override,
+                         int zb, int ze,
                          cudaStream_t stream, unsigned* dev_err,
                          LaunchInfo* info) {
   using C = StepTmaCfg<T, BY, S>;
@@ -342,29 +347,31 @@ cudaError_t launch_tma_t(const CUtensorMap& src, void* f2, int nx, int ny,
                                                 C::SMEM);
   const int gx = (nx + C::BX - 1) / C::BX;
   const int gy = (ny + BY - 1) / BY;
+  const int nzr = ze - zb;
   const int zchunk = zchunk_override > 0
                          ? zchunk_override
-                         : pick_zchunk(nz, (long)gx * gy, occ, 8);
-  const int gz = (nz + zchunk - 1) / zchunk;
+                         : pick_zchunk(nzr, (long)gx * gy, occ, 8);
+  const int gz = (nzr + zchunk - 1) / zchunk;
   if (info) *info = LaunchInfo{gx, gy, gz, C::THREADS, C::SMEM, zchunk, occ};
   kern<<<dim3(gx, gy, gz), C::THREADS, C::SMEM, stream>>>(
-      src, static_cast<T*>(f2), nx, ny, nz, coef_from<T>(coef), zchunk,
-      dev_err);
+      src, static_cast<T*>(f2), nx, ny, nz, coef_from<T>(coef), zchunk, zb,
+      ze, dev_err);
   return cudaGetLastError();
 }
 
 template <typename T, bool F>
 cudaError_t launch_tma_dtype(const CUtensorMap& src, void* f2, int nx, int ny,
                              int nz, const void* coef, int variant,
-                             int zchunk_override, cudaStream_t stream,
-                             unsigned* dev_err, LaunchInfo* info) {
+                             int zchunk_override, int zb, int ze,
+                             cudaStream_t stream, unsigned* dev_err,
+                             LaunchInfo* info) {
   switch (variant) {
-    case 0: return launch_tma_t<T, 32, 4, F>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
-    case 1: return launch_tma_t<T, 16, 4, F>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
-    case 2: return launch_tma_t<T, 8, 4, F>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
-    case 3: return launch_tma_t<T, 16, 6, F>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
-    case 4: return launch_tma_t<T, 32, 6, F>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
-    case 5: return launch_tma_t<T, 8, 8, F>(src, f2, nx, ny, nz, coef, zchunk_override, stream, dev_err, info);
+    case 0: return launch_tma_t<T, 32, 4, F>(src, f2, nx, ny, nz, coef, zchunk_override, zb, ze, stream, dev_err, info);
+    case 1: return launch_tma_t<T, 16, 4, F>(src, f2, nx, ny, nz, coef, zchunk_override, zb, ze, stream, dev_err, info);
+    case 2: return launch_tma_t<T, 8, 4, F>(src, f2, nx, ny, nz, coef, zchunk_override, zb, ze, stream, dev_err, info);
+    case 3: return launch_tma_t<T, 16, 6, F>(src, f2, nx, ny, nz, coef, zchunk_override, zb, ze, stream, dev_err, info);
+    case 4: return launch_tma_t<T, 32, 6, F>(src, f2, nx, ny, nz, coef, zchunk_override, zb, ze, stream, dev_err, info);
+    case 5: return launch_tma_t<T, 8, 8, F>(src, f2, nx, ny, nz, coef, zchunk_override, zb, ze, stream, dev_err, info);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -427,10 +434,12 @@ cudaError_t launch_step_tma(const CUtensorMap& src, void* f2, int nx, int ny,
                             int nz, const void* coef, int dtype, int variant,
                             int zchunk_override, int flip_y,
                             cudaStream_t stream, unsigned* dev_err,
-                            LaunchInfo* info) {
+                            LaunchInfo* info, int zb, int ze) {
+  if (ze < 0) ze = nz;
+  if (zb < 0 || zb >= ze || ze > nz) return cudaErrorInvalidValue;
   auto run = [&](auto fn) {
-    return fn(src, f2, nx, ny, nz, coef, variant, zchunk_override, stream,
-              dev_err, info);
+    return fn(src, f2, nx, ny, nz, coef, variant, zchunk_override, zb, ze,
+              stream, dev_err, info);
   };
   if (dtype == kF64)
     return flip_y ? run(launch_tma_dtype<double, true>)
@@ -442,17 +451,19 @@ cudaError_t launch_step_tma(const CUtensorMap& src, void* f2, int nx, int ny,
 cudaError_t launch_step_generic(const void* f1, void* f2, int nx, int ny,
                                 int nz, const void* coef, int dtype,
                                 int flip_y, cudaStream_t stream,
-                                LaunchInfo* info) {
+                                LaunchInfo* info, int zb, int ze) {
+  if (ze < 0) ze = nz;
+  if (zb < 0 || zb >= ze || ze > nz) return cudaErrorInvalidValue;
   const int bx = dtype == kF64 ? GenTile<double>::BX : GenTile<float>::BX;
   const int by = dtype == kF64 ? GenTile<double>::BY : GenTile<float>::BY;
   const int gx = (nx + bx - 1) / bx;
   const int gy = (ny + by - 1) / by;
-  const int zchunk = pick_zchunk(nz, (long)gx * gy, 8, 32);
-  const int gz = (nz + zchunk - 1) / zchunk;
+  const int zchunk = pick_zchunk(ze - zb, (long)gx * gy, 8, 32);
+  const int gz = (ze - zb + zchunk - 1) / zchunk;
   if (info) *info = LaunchInfo{gx, gy, gz, 256, 0, zchunk, 8};
   dim3 grid(gx, gy, gz), block(256);
   auto go = [&](auto kern, auto* a, auto* b, auto k) {
-    kern<<<grid, block, 0, stream>>>(a, b, nx, ny, nz, k, zchunk);
+    kern<<<grid, block, 0, stream>>>(a, b, nx, ny, nz, k, zchunk, zb, ze);
   };
   const double* d1 = static_cast<const double*>(f1);
   const float* s1 = static_cast<const float*>(f1);

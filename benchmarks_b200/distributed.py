@@ -4,17 +4,20 @@ The reference has no in-tree multi-node path (its only one is the external
 Physis MPI runtime, src/diffusion3d/Makefile:253-268).  Here each rank of a
 torch.distributed process group (NCCL over NVLink between GPUs) owns planes
 [z0, z1) of the global nx*ny*nz field plus up to `halo` ghost planes on each
-side that has a neighbour.  Every `halo` steps the ranks exchange their
-`halo` outermost owned planes with both neighbours (send/recv into the
-neighbours' ghost planes, landing in the receiver's own memory), then each
-rank runs `halo` ordinary steps on its local buffer with the single-grid
-kernels.  The local stencil clamps at the local buffer's edges; that is the
-reference's rule exactly at the global boundary, and at a ghost edge it
-corrupts one more ghost plane per step -- never an owned plane within
-`halo` steps.  So the owned planes are bit-identical to a single-GPU run.
+side that has a neighbour.  Planes move by send/recv into the
+neighbours' ghost planes, landing in the receiver's own memory (NCCL
+between GPUs; through host memory on gloo).  SlabSolver has two schedules
+(its docstring): an overlapped one that steps the two boundary planes
+first, exchanges them while the interior steps, and never computes a plane
+twice; and a halo-h one that exchanges h planes every h steps and runs the
+h steps on the whole local buffer in one call.  The local stencil clamps at
+the local buffer's edges; that is the reference's rule exactly at the
+global boundary, and at a ghost edge it corrupts one more ghost plane per
+step -- never an owned plane within h steps.  So the owned planes are
+bit-identical to a single-GPU run.
 
 Communication per exchange: 2 * halo planes of nx*ny values per interior
-rank boundary; compute overhead: 2 * halo extra planes per step.
+rank boundary.
 """
 from __future__ import annotations
 
@@ -67,37 +70,114 @@ class SlabDecomposition:
         return slice(self.z1 - self.lo, self.hi - self.lo)
 
 
+class SingleProcess:
+    """The process-group calls SlabSolver makes, for one rank alone (no
+    torch.distributed group): no neighbours, so nothing is exchanged."""
+
+    @staticmethod
+    def get_rank():
+        return 0
+
+    @staticmethod
+    def get_world_size():
+        return 1
+
+    @staticmethod
+    def get_backend():
+        return "nccl"
+
+    @staticmethod
+    def all_gather(parts, t):
+        parts[0].copy_(t)
+
+
+def _host_staged(dist, tensor):
+    """Whether send/recv of `tensor` must go through host memory: a CUDA
+    tensor on a backend without device transport (gloo)."""
+    return tensor.is_cuda and dist.get_backend() != "nccl"
+
+
+class _Exchange:
+    """Posted sends and receives of whole planes (contiguous slices of a
+    (planes, ny, nx) buffer).  On NCCL the planes move between GPUs, into
+    the receiver's own memory, on the library's stream, ordered after the
+    work already queued on the caller's stream; wait() orders the caller's
+    stream after them.  On gloo with CUDA tensors the planes are staged
+    through host memory (the send copies are taken when the exchange is
+    posted, the receive copies land in wait())."""
+
+    def __init__(self, dist, sends, recvs, group=None):
+        # sends / recvs: [(peer, tensor)]
+        self.dist = dist
+        self.recvs = recvs
+        self.staged = []
+        ops = []
+        for peer, t in sends:
+            if _host_staged(dist, t):
+                t = t.cpu()
+            ops.append(dist.P2POp(dist.isend, t, peer, group))
+        for peer, t in recvs:
+            if _host_staged(dist, t):
+                h = torch_empty_like_cpu(t)
+                self.staged.append((t, h))
+                t = h
+            ops.append(dist.P2POp(dist.irecv, t, peer, group))
+        self.reqs = dist.batch_isend_irecv(ops) if ops else []
+
+    def wait(self):
+        for r in self.reqs:
+            r.wait()
+        for dev, host in self.staged:
+            dev.copy_(host)
+
+
+def torch_empty_like_cpu(t):
+    import torch
+    return torch.empty(t.shape, dtype=t.dtype, device="cpu")
+
+
 def exchange(dist, field, dec, group=None):
     """Fills the ghost planes of `field` (local_nz, ny, nx) from the
     neighbours.  Every rank calls this the same number of times."""
-    ops = []
+    sends, recvs = [], []
     if dec.down is not None:
-        ops.append(dist.P2POp(dist.isend, field[dec.send_down()].contiguous(),
-                              dec.down, group))
-        rd = field[dec.recv_down()]
-        ops.append(dist.P2POp(dist.irecv, rd, dec.down, group))
+        sends.append((dec.down, field[dec.send_down()]))
+        recvs.append((dec.down, field[dec.recv_down()]))
     if dec.up is not None:
-        ops.append(dist.P2POp(dist.isend, field[dec.send_up()].contiguous(),
-                              dec.up, group))
-        ru = field[dec.recv_up()]
-        ops.append(dist.P2POp(dist.irecv, ru, dec.up, group))
-    if ops:
-        for req in dist.batch_isend_irecv(ops):
-            req.wait()
+        sends.append((dec.up, field[dec.send_up()]))
+        recvs.append((dec.up, field[dec.recv_up()]))
+    _Exchange(dist, sends, recvs, group).wait()
 
 
 class SlabSolver:
     """Runs `count` steps of one global field split across the group.
 
-    step_fn(src, dst) advances a local (local_nz, ny, nx) buffer by one
-    step; the default uses this rank's GPU through the C ABI
-    (Plan.step on the local buffer).
+    Two schedules, both bit-identical to a one-GPU run:
+    * overlap=True (halo 1): every step first computes the two owned planes
+      the neighbours need (d3d_step_planes), posts their exchange into the
+      neighbours' ghost planes of the output buffer, computes the interior
+      planes while the planes travel, then waits.  No plane is computed
+      twice.
+    * overlap=False (halo h >= 1): every h steps the ranks exchange their h
+      outermost owned planes, then each rank runs h steps on its whole
+      local buffer with one RunKernel-style call (the plan's kernels: fused
+      two-step passes where it uses them); the ghost planes are computed
+      redundantly and go stale one plane per step, never reaching an owned
+      plane within h steps.
+
+    step_fn(src, dst), when given, replaces the CUDA plan (one whole-buffer
+    step; overlap is then unavailable): the CPU tests pass the oracle's
+    step there.
     """
 
     def __init__(self, dist, nx, ny, nz, coeff, halo=1, step_fn=None,
-                 device=None, dtype=None):
+                 device=None, dtype=None, overlap=False):
         import torch
         self.dist = dist
+        if overlap and (halo != 1 or step_fn is not None):
+            raise ValueError("the overlapped schedule is halo 1 on the "
+                             "CUDA plan")
+        self.overlap = overlap
         self.dec = SlabDecomposition(nz, dist.get_rank(),
                                      dist.get_world_size(), halo)
         self.nx, self.ny, self.nz = nx, ny, nz
@@ -107,14 +187,11 @@ class SlabSolver:
         shape = (self.dec.local_nz, ny, nx)
         self.f1 = torch.zeros(shape, dtype=self.dtype, device=self.device)
         self.f2 = torch.zeros_like(self.f1)
+        self._plan = None
         if step_fn is None:
             from . import F32, F64, Plan
-            plan = Plan(nx, ny, self.dec.local_nz,
-                        F64 if self.dtype == torch.float64 else F32)
-            self._plan = plan
-
-            def step_fn(src, dst):
-                plan.step(src, dst, self.coeff)
+            self._plan = Plan(nx, ny, self.dec.local_nz,
+                              F64 if self.dtype == torch.float64 else F32)
         self.step_fn = step_fn
 
     def load(self, global_field):
@@ -123,15 +200,53 @@ class SlabSolver:
         g = torch.as_tensor(global_field)
         self.f1.copy_(g[self.dec.lo:self.dec.hi])
 
+    def _step_overlapped(self):
+        d, plan, c = self.dec, self._plan, self.coeff
+        f1, f2 = self.f1, self.f2
+        lo, hi = d.z0 - d.lo, d.z1 - d.lo  # owned planes, local indices
+        edge = []
+        if d.down is not None:
+            edge.append(lo)
+        if d.up is not None and hi - 1 not in edge:
+            edge.append(hi - 1)
+        for z in edge:
+            plan.step_planes(f1, f2, z, z + 1, c)
+        sends, recvs = [], []
+        if d.down is not None:
+            sends.append((d.down, f2[lo:lo + 1]))
+            recvs.append((d.down, f2[lo - 1:lo]))
+        if d.up is not None:
+            sends.append((d.up, f2[hi - 1:hi]))
+            recvs.append((d.up, f2[hi:hi + 1]))
+        if any(_host_staged(self.dist, t) for _, t in sends):
+            import torch
+            torch.cuda.synchronize(self.device)
+        xchg = _Exchange(self.dist, sends, recvs)
+        ilo = lo + (1 if d.down is not None else 0)
+        ihi = hi - (1 if d.up is not None else 0)
+        if ilo < ihi:
+            plan.step_planes(f1, f2, ilo, ihi, c)
+        xchg.wait()
+        self.f1, self.f2 = f2, f1
+
     def run(self, count):
+        if self.overlap:
+            for _ in range(count):
+                self._step_overlapped()
+            return self.f1[self.dec.owned()]
         h = self.dec.halo
         done = 0
         while done < count:
             exchange(self.dist, self.f1, self.dec)
-            for _ in range(min(h, count - done)):
-                self.step_fn(self.f1, self.f2)
-                self.f1, self.f2 = self.f2, self.f1
-                done += 1
+            k = min(h, count - done)
+            if self.step_fn is not None:
+                for _ in range(k):
+                    self.step_fn(self.f1, self.f2)
+                    self.f1, self.f2 = self.f2, self.f1
+            else:
+                a, b = self._plan.run(self.f1, self.f2, k, self.coeff)
+                self.f1, self.f2 = a, b
+            done += k
         return self.f1[self.dec.owned()]
 
     def gather(self):
@@ -141,9 +256,16 @@ class SlabSolver:
         sizes = [slab_bounds(self.nz, r, self.dec.world)
                  for r in range(self.dec.world)]
         maxn = max(z1 - z0 for z0, z1 in sizes)
+        staged = _host_staged(self.dist, owned)
+        dev = torch.device("cpu") if staged else self.device
         pad = torch.zeros((maxn, self.ny, self.nx), dtype=self.dtype,
-                          device=self.device)
-        pad[:owned.shape[0]] = owned
+                          device=dev)
+        pad[:owned.shape[0]] = owned.to(dev)
         parts = [torch.empty_like(pad) for _ in sizes]
         self.dist.all_gather(parts, pad)
         return torch.cat([p[:z1 - z0] for p, (z0, z1) in zip(parts, sizes)])
+
+    def close(self):
+        if self._plan is not None:
+            self._plan.close()
+            self._plan = None

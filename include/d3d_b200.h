@@ -154,6 +154,15 @@ int d3d_stream_sync(void* stream);
 int d3d_step(d3d_plan plan, const void* f1, void* f2, const void* coeff,
              void* stream);
 
+/* d3d_step restricted to output planes [z_begin, z_end) of a 3D plan
+ * (0 <= z_begin < z_end <= nz): those planes of f2 get one step of f1, the
+ * rest of f2 is not touched; neighbours and the replicated boundary are
+ * the whole field's.  No counterpart in the reference (its RunKernel steps
+ * whole fields); the z-slab solver runs the planes its neighbours need
+ * first, hands them to the exchange, and steps the interior meanwhile. */
+int d3d_step_planes(d3d_plan plan, const void* f1, void* f2, int z_begin,
+                    int z_end, const void* coeff, void* stream);
+
 /* `count` time steps ping-ponging between two device buffers: the launch
  * loop of Diffusion3DCUDA::RunKernel (diffusion3d_cuda.cu:361-367).  Like
  * the reference, the buffer pointers are swapped after every step, so on
@@ -277,8 +286,23 @@ int d3d_batch_autotune(d3d_batch batch, void* stream);
  * kernel with 1 or 2 segments a thread (4 is the default before
  * d3d_batch_autotune); 6 and 7 its two-step form (temporal-block depth 2:
  * fused step pairs, and one strip step to finish an odd step count),
- * D3D_E_UNSUPPORTED if a grid is wider than 248 floats. */
+ * D3D_E_UNSUPPORTED if a grid is wider than 248 floats.  Kind 8
+ * (D3D_BATCH_KIND_RESIDENT) runs every grid that fits on the cluster-
+ * resident kernel: a cluster of up to 16 CTAs holds the whole grid in
+ * shared memory for all of its steps (one persistent launch per cluster
+ * size and thread shape, walking its grids through a work counter); the
+ * grids it does not fit take kind 4.  d3d_batch_autotune also times the
+ * whole run with and without kind 8 and keeps the faster. */
+#define D3D_BATCH_NUM_KINDS 9
+#define D3D_BATCH_KIND_RESIDENT 8
 int d3d_batch_set_kind(d3d_batch batch, int kind);
+
+/* Per-grid step counters of the last run (n = the batch's grid count):
+ * the cluster-resident kernel advances a grid's counter after each of its
+ * steps; grids on the per-step kinds get their step count once their last
+ * launch has run.  A counter below the grid's steps after a run has
+ * returned names a grid whose steps did not all complete.  Synchronous. */
+int d3d_batch_progress(d3d_batch batch, int* steps_done, int n);
 
 /* Runs every grid for its step count: the first call captures the run
  * into a CUDA graph, every call replays it as one graph launch.

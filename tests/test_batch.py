@@ -158,12 +158,13 @@ def test_autotuned_batch_still_bit_exact():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kind", range(8))
+@pytest.mark.parametrize("kind", range(B.BATCH_NUM_KINDS))
 def test_every_kernel_kind_bit_exact(kind):
-    """Each march tile shape, both strip forms and both two-step strip
-    forms on grids of every size class, nx leaving 0..3 pad columns in the
-    pitched copies (nx = 1 included), zero-step grids, odd and even step
-    counts (a two-step class ends odd counts with one strip step)."""
+    """Each march tile shape, both strip forms, both two-step strip forms
+    and the cluster-resident kernel on grids of every size class, nx
+    leaving 0..3 pad columns in the pitched copies (nx = 1 included),
+    zero-step grids, odd and even step counts (a two-step class ends odd
+    counts with one strip step)."""
     dims = [(1, 1, 1), (1, 5, 7), (3, 2, 9), (17, 23, 5), (24, 9, 13),
             (25, 30, 2), (40, 41, 11), (41, 3, 6), (72, 17, 8), (73, 70, 9),
             (96, 96, 4), (13, 1, 30)]
@@ -237,4 +238,81 @@ def test_more_grids_than_one_launch_row():
         want = O.run(fields[i % 6], c, steps)
         assert batch.result(i).cpu().numpy().tobytes() == want.tobytes(), i
     assert B.check_device_errors() == 0
+    batch.close()
+
+
+# Grids for the cluster-resident kernel.  A CTA holds at most 57,856 floats:
+# pc planes of ceil4(nx) * ny and one halo plane, so a grid needs
+# ceil(nz / (57856 // plane - 1)) CTAs.  These cover clusters of 1 to 16
+# CTAs, a last CTA with fewer planes, one-plane slabs, every thread shape
+# (plane segments up to 256, 512, 1024, 2048 and 2304), rows of one
+# segment, nx leaving 0..3 pad columns, and grids it does not fit (too
+# many CTAs; too many segments a plane), which run on the strip kind.
+RESIDENT_DIMS = [(1, 1, 1), (5, 1, 9), (17, 23, 5), (13, 1, 30),
+                 (64, 64, 64), (88, 80, 37), (96, 96, 80), (95, 7, 300),
+                 (33, 60, 45), (96, 90, 12), (40, 40, 200), (96, 96, 96),
+                 (100, 96, 10), (57, 31, 128), (16, 96, 96), (96, 16, 3)]
+
+
+def _resident_specs(steps_of):
+    return [(nx, ny, nz, steps_of(i),
+             B.batch_coefficients(nx, ny, nz, 0.05 + 0.01 * i))
+            for i, (nx, ny, nz) in enumerate(RESIDENT_DIMS)]
+
+
+@pytest.mark.gpu
+def test_cluster_resident_kind_bit_exact_with_step_counters():
+    specs = _resident_specs(lambda i: 1 + (i * 7) % 12)
+    fields = _fields(specs, 1300)
+    outs, batch = _run_batch(specs, fields, kind=B.BATCH_KIND_RESIDENT)
+    for (nx, ny, nz, steps, c), f, o in zip(specs, fields, outs):
+        assert o.tobytes() == O.run(f, c, steps).tobytes(), (nx, ny, nz,
+                                                              steps)
+    assert B.check_device_errors() == 0
+    info = batch.info()
+    res = info["resident"]
+    assert res["on"]
+    # (96, 96, 96) needs 20 CTAs and (100, 96, 10) 2400 segments a plane:
+    # those two run on the strip kind, every other grid on the resident one
+    assert res["grids"] == len(specs) - 2
+    clusters = {c["cluster"] for c in res["classes"]}
+    assert 1 in clusters and 16 in clusters
+    assert {c["threads"] for c in res["classes"]} == {128, 256, 512, 384}
+    # every grid's counter reached its step count
+    assert list(batch.progress()) == [s for _, _, _, s, _ in specs]
+    batch.close()
+
+
+@pytest.mark.gpu
+def test_cluster_resident_same_alone_and_in_the_mix():
+    specs = _resident_specs(lambda i: 3 + i % 5)
+    fields = _fields(specs, 1400)
+    mixed, _ = _run_batch(specs, fields, kind=B.BATCH_KIND_RESIDENT)
+    for i in (0, 4, 6, 7, 11):
+        alone, _ = _run_batch([specs[i]], [fields[i]],
+                              kind=B.BATCH_KIND_RESIDENT)
+        assert alone[0].tobytes() == mixed[i].tobytes(), i
+
+
+@pytest.mark.gpu
+def test_cluster_resident_replays_and_long_runs():
+    """The captured graph replays (work counters reset each run), and a
+    few hundred steps keep the bits of the oracle's run."""
+    torch = pytest.importorskip("torch")
+    specs = [(48, 40, 36, 301, B.batch_coefficients(48, 40, 36, 0.1)),
+             (96, 64, 70, 257, B.batch_coefficients(96, 64, 70, 0.1)),
+             (23, 19, 11, 500, B.batch_coefficients(23, 19, 11, 0.1))]
+    fields = _fields(specs, 1500)
+    batch = B.Batch(specs)
+    batch.set_kind(B.BATCH_KIND_RESIDENT)
+    for _ in range(2):
+        for i, f in enumerate(fields):
+            batch.input(i).copy_(torch.from_numpy(f))
+        batch.run()
+        torch.cuda.synchronize()
+        for i, ((nx, ny, nz, steps, c), f) in enumerate(zip(specs, fields)):
+            assert batch.result(i).cpu().numpy().tobytes() == \
+                O.run(f, c, steps).tobytes(), i
+        assert list(batch.progress()) == [s for _, _, _, s, _ in specs]
+    assert batch.info()["launches_per_run"] < 10
     batch.close()

@@ -1,9 +1,13 @@
 """Multi-rank paths on CPU (gloo, 127.0.0.1), no GPU needed.
 
 * z-slab decomposition with halo exchange: ranks run the oracle's step on
-  their local slab (the CUDA kernels take that role on GPUs); the gathered
-  field must be bit-identical to a single-process run, for several world
-  sizes, halo depths and uneven slabs.
+  their local slab; the gathered field must be bit-identical to a
+  single-process run, for several world sizes, halo depths and uneven
+  slabs.
+* (GPU) the same with the CUDA kernels: 2 or 3 gloo ranks share one GPU,
+  each stepping its slab through the C ABI (the overlapped schedule with
+  d3d_step_planes, and the halo-h schedule with whole-buffer runs), the
+  planes staged through host memory; no kernel waits on another rank's.
 * bench-style max-over-ranks timing reduction.
 """
 import os
@@ -110,6 +114,96 @@ def test_slab_solver_matches_single_process(tmp_path, world, halo, dims,
     assert full.tobytes() == O.run(field, c, count).tobytes()
 
 
+def _slab_cuda_worker(rank, world, port, nx, ny, nz, count, halo, overlap,
+                      seed, out):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    import oracle as O
+    from benchmarks_b200.distributed import SlabSolver
+
+    torch.cuda.set_device(0)
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=timedelta(seconds=60))
+    try:
+        c, _ = O.params(nx, ny, nz)
+        field = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), seed)
+        solver = SlabSolver(dist, nx, ny, nz, c, halo=halo, overlap=overlap)
+        solver.load(torch.from_numpy(field).cuda())
+        solver.run(count)
+        torch.cuda.synchronize()
+        full = solver.gather().cpu().numpy()
+        solver.close()
+        if rank == 0:
+            np.save(out, full)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("world,halo,overlap,dims,count", [
+    (2, 1, True, (64, 40, 36), 9),
+    (3, 1, True, (136, 17, 23), 6),
+    (2, 2, False, (64, 40, 36), 9),
+    (2, 3, False, (130, 24, 31), 7),
+])
+def test_slab_solver_cuda_kernels_across_ranks(tmp_path, world, halo, overlap,
+                                               dims, count):
+    """Ranks on one GPU, exchange through host memory (gloo): the gathered
+    field equals the oracle's run and the one-GPU run, bit for bit."""
+    import torch
+    import torch.multiprocessing as mp
+
+    import benchmarks_b200 as B
+    import oracle as O
+    nx, ny, nz = dims
+    out = str(tmp_path / "full.npy")
+    mp.start_processes(_slab_cuda_worker,
+                       args=(world, _free_port(), nx, ny, nz, count, halo,
+                             overlap, 6, out),
+                       nprocs=world, join=True, start_method="spawn")
+    full = np.load(out)
+    c, _ = O.params(nx, ny, nz)
+    field = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), 6)
+    assert full.tobytes() == O.run(field, c, count).tobytes()
+    plan = B.Plan(nx, ny, nz)
+    f1 = torch.from_numpy(field).cuda()
+    res, _ = plan.run(f1, torch.empty_like(f1), count, c)
+    assert res.cpu().numpy().tobytes() == full.tobytes()
+    plan.close()
+
+
+@pytest.mark.gpu
+def test_step_planes_writes_only_its_planes():
+    """d3d_step_planes: the planes asked for equal a whole step's, the
+    others keep their contents; bad ranges are refused."""
+    import torch
+
+    import benchmarks_b200 as B
+    import oracle as O
+    for dims in ((128, 24, 20), (37, 11, 9)):  # TMA and generic paths
+        nx, ny, nz = dims
+        c, _ = O.params(nx, ny, nz)
+        fin = O.seeded_noise((nz, ny, nx), 8, amplitude=1.0)
+        ref = O.run(fin, c, 1)
+        plan = B.Plan(nx, ny, nz)
+        f1 = torch.from_numpy(fin).cuda()
+        for zb, ze in ((0, 1), (nz - 1, nz), (3, 7), (0, nz), (1, nz - 1)):
+            f2 = torch.full_like(f1, -5.0)
+            plan.step_planes(f1, f2, zb, ze, c)
+            got = f2.cpu().numpy()
+            assert got[zb:ze].tobytes() == ref[zb:ze].tobytes(), (dims, zb)
+            assert (got[:zb] == -5.0).all() and (got[ze:] == -5.0).all()
+        for zb, ze in ((-1, 2), (3, 3), (0, nz + 1)):
+            with pytest.raises(B.D3DError) as ei:
+                plan.step_planes(f1, f2, zb, ze, c)
+            assert ei.value.code == B.D3D_E_INVALID
+        plan.close()
+
+
 @pytest.mark.gpu
 def test_slab_solver_cuda_kernels_world_one():
     """The default step (our CUDA kernels through the C ABI) inside the slab
@@ -128,11 +222,16 @@ def test_slab_solver_cuda_kernels_world_one():
     dist.init_process_group("nccl", store=store, rank=0, world_size=1,
                             timeout=timedelta(seconds=60))
     try:
-        solver = SlabSolver(dist, nx, ny, nz, c, halo=2)
-        solver.load(torch.from_numpy(field).cuda())
-        solver.run(count)
-        torch.cuda.synchronize()
-        full = solver.gather().cpu().numpy()
+        fulls = []
+        for halo, overlap in ((2, False), (1, True)):
+            solver = SlabSolver(dist, nx, ny, nz, c, halo=halo,
+                                overlap=overlap)
+            solver.load(torch.from_numpy(field).cuda())
+            solver.run(count)
+            torch.cuda.synchronize()
+            fulls.append(solver.gather().cpu().numpy())
+            solver.close()
     finally:
         dist.destroy_process_group()
-    assert full.tobytes() == O.run(field, c, count).tobytes()
+    for full in fulls:
+        assert full.tobytes() == O.run(field, c, count).tobytes()
