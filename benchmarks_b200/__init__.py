@@ -81,6 +81,7 @@ _SIGNATURES = {
     "d3d_batch_info": ([_vp, ctypes.c_char_p, _sz], _i),
     "d3d_batch_progress": ([_vp, ctypes.POINTER(ctypes.c_int), _i], _i),
     "d3d_batch_destroy": ([_vp], _i),
+    "d3d_server_set_resident": ([_vp, _i], _i),
     "d3d_server_create": ([_sz, _i, _vpp], _i),
     "d3d_server_submit": ([_vp, _i, _i, _i, _i,
                            ctypes.POINTER(ctypes.c_float), _vp, _vp,
@@ -521,7 +522,8 @@ class Server:
     asynchronous copies); tick() runs one scheduling round and returns the
     ids that finished."""
 
-    def __init__(self, arena_bytes, chunk=8, kernel=None, lanes=None):
+    def __init__(self, arena_bytes, chunk=8, kernel=None, lanes=None,
+                 resident=None):
         h = ctypes.c_void_p()
         check(lib().d3d_server_create(int(arena_bytes), chunk,
                                       ctypes.byref(h)))
@@ -530,6 +532,8 @@ class Server:
             self.set_kernel(kernel)
         if lanes is not None:
             self.set_lanes(lanes)
+        if resident is not None:
+            self.set_resident(resident)
         self._keep = {}
         self._ids = (ctypes.c_longlong * 4096)()
 
@@ -565,6 +569,11 @@ class Server:
     def set_lanes(self, lanes):
         """Compute streams of the idle server (1..4, default 4)."""
         check(lib().d3d_server_set_lanes(self._h, int(lanes)))
+
+    def set_resident(self, on):
+        """Whether the idle server runs the solves that fit it on the
+        cluster-resident kernel (default on)."""
+        check(lib().d3d_server_set_resident(self._h, int(bool(on))))
 
     def pending(self):
         q, a, r = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

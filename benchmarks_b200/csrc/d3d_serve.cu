@@ -10,6 +10,13 @@
 // At most two ticks are in flight; their descriptor/work lists use
 // alternating staging buffers.
 //
+// Small solves.  A solve that the cluster-resident kernel fits (its whole
+// grid in the shared memory of one cluster of at most 16 CTAs,
+// d3d_resident.cu) skips the ticks: it is admitted into one dense buffer,
+// and the next tick launches every such solve admitted since the last one
+// in one persistent launch per cluster size, which runs all of their steps;
+// each result is copied out as soon as that launch ends.
+//
 // Step kernel.  By default the strip form of the pitched TMA kernel
 // (d3d_pitched.cu): each solve is stored with rows padded to a 16-byte
 // pitch and read through two tensor maps encoded at admission, whose box
@@ -23,6 +30,7 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <tuple>
 #include <vector>
 
 #include "d3d_b200.h"
@@ -92,6 +100,11 @@ class ArenaAlloc {
 struct Request {
   CUtensorMap map[2];  // pitched kernel: the fields at off_a and off_b
   long long id;
+  // Cluster-resident solve: one dense buffer (off_a), its launch class
+  // (cluster size, thread shape) and shared memory, planes per CTA.
+  bool resident = false;
+  int r_cluster = 0, r_variant = 0, r_pc = 0;
+  size_t r_smem = 0;
   int nx, ny, nz, steps, done;
   int px;  // row pitch in floats (nx, or nx rounded up to 4 when pitched)
   d3d::StripShape strip{};  // strip kernels: pieces, segments, rows
@@ -108,6 +121,21 @@ struct Request {
     return (unsigned long long)px * ny * nz;
   }
 };
+
+// Staging of one group of cluster-resident solves: descriptors (pinned and
+// device), one work counter per launch, one step counter per solve, and
+// the event that ends the group's launches.
+struct ResStaging {
+  d3d::ResidentDesc* h = nullptr;
+  d3d::ResidentDesc* d = nullptr;
+  int* d_steps = nullptr;
+  size_t cap = 0;
+  unsigned* d_queue = nullptr;  // kMaxResClasses counters
+  cudaEvent_t done = nullptr;
+  bool in_flight = false;
+};
+constexpr int kMaxResClasses =
+    d3d::kResidentMaxCluster * d3d::kNumResidentVariants;
 
 // Staging for one tick's descriptors (BatchDesc or PitchedDesc, by the
 // server's kernel) and work items, pinned + device.
@@ -147,6 +175,15 @@ struct d3d_server_s {
   long long submitted = 0, completed = 0, ticks = 0;
   double step_ms = 0.0;  // device time of the step launches
   unsigned long long launches = 0, peak_used = 0;
+  // Cluster-resident solves: admitted and waiting for the next group
+  // launch; the stream and stagings of those launches.
+  bool resident = true;
+  std::vector<Request*> res_pending;
+  cudaStream_t res_stream = nullptr;
+  ResStaging rstage[2];
+  int res_index = 0;
+  long long res_solves = 0, res_launches = 0;
+  std::map<std::tuple<int, int, size_t>, int> res_max_clusters;
 };
 
 namespace {
@@ -185,8 +222,59 @@ void free_request(d3d_server s, Request* r) {
   if (r->ev_in) cudaEventDestroy(r->ev_in);
   if (r->ev_out) cudaEventDestroy(r->ev_out);
   s->alloc.release(r->off_a, r->elems());
-  s->alloc.release(r->off_b, r->elems());
+  if (!r->resident) s->alloc.release(r->off_b, r->elems());
   delete r;
+}
+
+// Clusters of one resident launch class that fit the GPU at once (0: not
+// schedulable), cached per (thread shape, cluster size, shared memory).
+int res_max_clusters(d3d_server s, int variant, int cluster, size_t smem) {
+  const auto key = std::make_tuple(variant, cluster, smem);
+  auto it = s->res_max_clusters.find(key);
+  if (it != s->res_max_clusters.end()) return it->second;
+  int n = 0;
+  if (d3d::resident_max_clusters(variant, cluster, smem, &n) != cudaSuccess) {
+    cudaGetLastError();
+    n = 0;
+  }
+  s->res_max_clusters[key] = n;
+  return n;
+}
+
+// Whether a solve fits the cluster-resident kernel, and its class: the
+// same rule as the batch API's (a thread shape covering its ceil(nx/4) * ny
+// row segments a plane; at most 16 CTAs of pc planes plus one halo plane
+// each), on a cluster the GPU can schedule.
+void plan_resident_solve(d3d_server s, Request* r) {
+  r->resident = false;
+  if (!s->resident || r->steps < 1) return;
+  if (d3d::resident_prepare() != cudaSuccess) {
+    cudaGetLastError();
+    s->resident = false;
+    return;
+  }
+  const int px = (r->nx + 3) / 4 * 4, segs = px / 4;
+  const long long plane = (long long)px * r->ny;
+  const long long units = (long long)segs * r->ny;
+  int v = -1;
+  for (int j = 0; j < d3d::kNumResidentVariants && v < 0; ++j) {
+    const d3d::ResidentVariant& rv = d3d::resident_variant(j);
+    if (units <= (long long)rv.threads * rv.units) v = j;
+  }
+  if (v < 0) return;
+  const long long pmax = (long long)(d3d::kResidentSmemMax / 4) / plane - 1;
+  if (pmax < 1) return;
+  const int cl = (int)((r->nz + pmax - 1) / pmax);
+  if (cl > d3d::kResidentMaxCluster) return;
+  const int pc = (r->nz + cl - 1) / cl;
+  const size_t smem = (size_t)((pc + 1) * plane * 4);
+  if (res_max_clusters(s, v, cl, smem) < 1) return;
+  r->resident = true;
+  r->r_cluster = cl;
+  r->r_variant = v;
+  r->r_pc = pc;
+  r->r_smem = smem;
+  r->px = r->nx;  // one dense buffer
 }
 
 size_t dense_bytes(const Request* r) {
@@ -235,6 +323,22 @@ int admit(d3d_server s) {
   for (auto it = s->queued.begin(); it != s->queued.end();) {
     Request* r = *it;
     unsigned long long a, b;
+    if (r->resident) {
+      if (!s->alloc.alloc(r->elems(), &a)) {
+        ++it;
+        continue;
+      }
+      r->off_a = a;
+      S_TRY(cudaMemcpyAsync(s->arena + a, r->host_in, dense_bytes(r),
+                            cudaMemcpyHostToDevice, s->copy),
+            "H2D copy (input)");
+      S_TRY(cudaEventCreateWithFlags(&r->ev_in, cudaEventDisableTiming),
+            "cudaEventCreate");
+      S_TRY(cudaEventRecord(r->ev_in, s->copy), "cudaEventRecord");
+      it = s->queued.erase(it);
+      s->res_pending.push_back(r);
+      continue;
+    }
     if (!s->alloc.alloc(r->elems(), &a)) {
       ++it;
       continue;
@@ -298,6 +402,110 @@ int admit(d3d_server s) {
     }
   }
   s->peak_used = std::max(s->peak_used, s->alloc.used());
+  return D3D_OK;
+}
+
+// Launches every cluster-resident solve admitted since the last group:
+// one persistent launch per (cluster size, thread shape), largest work
+// first, on the resident stream after the solves' input copies; each
+// result is copied out once the group's launches end.
+int launch_resident_group(d3d_server s) {
+  if (s->res_pending.empty()) return D3D_OK;
+  ResStaging& st = s->rstage[s->res_index & 1];
+  if (st.in_flight) {
+    S_TRY(cudaEventSynchronize(st.done), "cudaEventSynchronize");
+    st.in_flight = false;
+  }
+  std::vector<Request*>& list = s->res_pending;
+  std::stable_sort(list.begin(), list.end(), [](const Request* x,
+                                                const Request* y) {
+    if (x->r_cluster != y->r_cluster) return x->r_cluster > y->r_cluster;
+    if (x->r_variant != y->r_variant) return x->r_variant < y->r_variant;
+    return (double)x->nx * x->ny * x->nz * x->steps >
+           (double)y->nx * y->ny * y->nz * y->steps;
+  });
+  const size_t n = list.size();
+  if (n > st.cap) {
+    if (st.h) cudaFreeHost(st.h);
+    if (st.d) cudaFree(st.d);
+    if (st.d_steps) cudaFree(st.d_steps);
+    st.h = nullptr;
+    st.d = nullptr;
+    st.d_steps = nullptr;
+    st.cap = std::max(n, 2 * st.cap);
+    S_TRY(cudaMallocHost(&st.h, st.cap * sizeof(d3d::ResidentDesc)),
+          "cudaMallocHost (resident staging)");
+    S_TRY(cudaMalloc(&st.d, st.cap * sizeof(d3d::ResidentDesc)),
+          "cudaMalloc (resident staging)");
+    S_TRY(cudaMalloc(&st.d_steps, st.cap * sizeof(int)),
+          "cudaMalloc (resident step counters)");
+  }
+  if (!st.d_queue) {
+    S_TRY(cudaMalloc(&st.d_queue, kMaxResClasses * sizeof(unsigned)),
+          "cudaMalloc (resident work counters)");
+    S_TRY(cudaEventCreateWithFlags(&st.done, cudaEventDisableTiming),
+          "cudaEventCreate");
+  }
+  for (size_t i = 0; i < n; ++i) {
+    const Request* r = list[i];
+    d3d::ResidentDesc& d = st.h[i];
+    d.in = s->arena + r->off_a;
+    d.out = s->arena + r->off_a;  // each CTA writes only the planes it read
+    d.nx = r->nx;
+    d.ny = r->ny;
+    d.nz = r->nz;
+    d.steps = r->steps;
+    d.px = (r->nx + 3) / 4 * 4;
+    d.segs = d.px / 4;
+    d.pc = r->r_pc;
+    d.grid_id = (int)i;
+    for (int j = 0; j < 7; ++j) d.k[j] = r->coeff[j];
+    d.k[7] = -0.0f;
+    S_TRY(cudaStreamWaitEvent(s->res_stream, r->ev_in, 0),
+          "cudaStreamWaitEvent");
+  }
+  cudaStream_t rs = s->res_stream;
+  S_TRY(cudaMemcpyAsync(st.d, st.h, n * sizeof(d3d::ResidentDesc),
+                        cudaMemcpyHostToDevice, rs),
+        "H2D resident descriptors");
+  S_TRY(cudaMemsetAsync(st.d_queue, 0, kMaxResClasses * sizeof(unsigned),
+                        rs),
+        "work counter reset");
+  int ci = 0;
+  for (size_t b = 0; b < n; ++ci) {
+    size_t e = b;
+    size_t smem = 0;
+    while (e < n && list[e]->r_cluster == list[b]->r_cluster &&
+           list[e]->r_variant == list[b]->r_variant) {
+      smem = std::max(smem, list[e]->r_smem);
+      ++e;
+    }
+    const int cl = list[b]->r_cluster, v = list[b]->r_variant;
+    const int nclusters =
+        std::min<int>((int)(e - b), res_max_clusters(s, v, cl, smem));
+    S_TRY(d3d::launch_resident(v, st.d + b, (int)(e - b), st.d_queue + ci,
+                               st.d_steps, cl, nclusters, smem, rs),
+          "resident launch");
+    ++s->res_launches;
+    ++s->launches;
+    d3d::note_launches(1);
+    b = e;
+  }
+  S_TRY(cudaEventRecord(st.done, rs), "cudaEventRecord");
+  st.in_flight = true;
+  ++s->res_index;
+  S_TRY(cudaStreamWaitEvent(s->copy, st.done, 0), "cudaStreamWaitEvent");
+  for (Request* r : list) {
+    S_TRY(cudaMemcpyAsync(r->host_out, s->arena + r->off_a, dense_bytes(r),
+                          cudaMemcpyDeviceToHost, s->copy),
+          "D2H copy (result)");
+    S_TRY(cudaEventCreateWithFlags(&r->ev_out, cudaEventDisableTiming),
+          "cudaEventCreate");
+    S_TRY(cudaEventRecord(r->ev_out, s->copy), "cudaEventRecord");
+    s->retiring.push_back(r);
+    ++s->res_solves;
+  }
+  list.clear();
   return D3D_OK;
 }
 
@@ -548,6 +756,8 @@ int d3d_server_create(size_t arena_bytes, int chunk, d3d_server* out) {
     e = cudaStreamCreateWithFlags(&s->lane[l], cudaStreamNonBlocking);
   if (e == cudaSuccess)
     e = cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking);
+  if (e == cudaSuccess)
+    e = cudaStreamCreateWithFlags(&s->res_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     d3d_server_destroy(s);
     return d3d::set_cuda_error(e, "server setup");
@@ -566,19 +776,23 @@ int d3d_server_submit(d3d_server s, int nx, int ny, int nz, int steps,
       ((long long)nx + 3) / 4 * 4 * ny >= (1LL << 31))
     return sfail(D3D_E_INVALID, "bad grid dimensions or steps");
   const int px = s->kernel >= 0 ? (nx + 3) / 4 * 4 : nx;
-  const unsigned long long pts = (unsigned long long)px * ny * nz;
-  const unsigned long long need = 2 * ((pts + kAlign - 1) / kAlign * kAlign);
-  if (need > s->arena_elems)
-    return sfail(D3D_E_BUSY, "solve larger than the server's arena");
   Request* r = new (std::nothrow) Request();
   if (!r) return sfail(D3D_E_OOM, "request allocation");
-  r->id = s->next_id++;
   r->px = px;
   r->nx = nx;
   r->ny = ny;
   r->nz = nz;
   r->steps = steps;
   r->done = 0;
+  plan_resident_solve(s, r);  // may switch it to one dense buffer
+  const unsigned long long pts = r->elems();
+  const unsigned long long need = (r->resident ? 1 : 2) *
+                                  ((pts + kAlign - 1) / kAlign * kAlign);
+  if (need > s->arena_elems) {
+    delete r;
+    return sfail(D3D_E_BUSY, "solve larger than the server's arena");
+  }
+  r->id = s->next_id++;
   memcpy(r->coeff, coeff, sizeof r->coeff);
   r->host_in = host_in;
   r->host_out = host_out;
@@ -614,9 +828,21 @@ int d3d_server_tick(d3d_server s, long long* done_ids, int max_done,
   // 2. admit, 3. advance (4. inside advance)
   int rc = admit(s);
   if (rc) return rc;
+  rc = launch_resident_group(s);
+  if (rc) return rc;
   rc = advance(s);
   if (rc) return rc;
   ++s->ticks;
+  return D3D_OK;
+}
+
+int d3d_server_set_resident(d3d_server s, int on) {
+  if (!s) return sfail(D3D_E_INVALID, "NULL server");
+  if (!s->queued.empty() || !s->active.empty() || !s->retiring.empty() ||
+      !s->res_pending.empty())
+    return sfail(D3D_E_BUSY,
+                 "the resident path changes only on an idle server");
+  s->resident = on != 0;
   return D3D_OK;
 }
 
@@ -624,7 +850,8 @@ int d3d_server_set_kernel(d3d_server s, int kernel) {
   if (!s) return sfail(D3D_E_INVALID, "NULL server");
   if (kernel < -1 || kernel > kMaxKernel)
     return sfail(D3D_E_INVALID, "no such server kernel");
-  if (!s->queued.empty() || !s->active.empty() || !s->retiring.empty())
+  if (!s->queued.empty() || !s->active.empty() || !s->retiring.empty() ||
+      !s->res_pending.empty())
     return sfail(D3D_E_BUSY, "the step kernel changes only on an idle server");
   s->kernel = kernel;
   return D3D_OK;
@@ -634,7 +861,8 @@ int d3d_server_set_lanes(d3d_server s, int lanes) {
   if (!s) return sfail(D3D_E_INVALID, "NULL server");
   if (lanes < 1 || lanes > kMaxLanes)
     return sfail(D3D_E_INVALID, "lanes must be 1 to 4");
-  if (!s->queued.empty() || !s->active.empty() || !s->retiring.empty())
+  if (!s->queued.empty() || !s->active.empty() || !s->retiring.empty() ||
+      !s->res_pending.empty())
     return sfail(D3D_E_BUSY, "lanes change only on an idle server");
   s->lanes = lanes;
   return D3D_OK;
@@ -644,7 +872,7 @@ int d3d_server_pending(d3d_server s, int* queued, int* active,
                        int* retiring) {
   if (!s) return sfail(D3D_E_INVALID, "NULL server");
   if (queued) *queued = (int)s->queued.size();
-  if (active) *active = (int)s->active.size();
+  if (active) *active = (int)(s->active.size() + s->res_pending.size());
   if (retiring) *retiring = (int)s->retiring.size();
   return D3D_OK;
 }
@@ -656,10 +884,13 @@ int d3d_server_stats(d3d_server s, char* buf, size_t len) {
            "{\"submitted\": %lld, \"completed\": %lld, \"ticks\": %lld, "
            "\"launches\": %llu, \"chunk\": %d, \"kernel\": %d, "
            "\"lanes\": %d, "
-           "\"step_ms\": %.4f, "
+           "\"step_ms\": %.4f, \"resident\": %s, "
+           "\"resident_solves\": %lld, \"resident_launches\": %lld, "
            "\"arena_bytes\": %llu, \"peak_arena_bytes\": %llu}",
            s->submitted, s->completed, s->ticks, s->launches, s->chunk,
-           s->kernel, s->lanes, s->step_ms, s->arena_elems * 4ULL, s->peak_used * 4ULL);
+           s->kernel, s->lanes, s->step_ms, s->resident ? "true" : "false",
+           s->res_solves, s->res_launches, s->arena_elems * 4ULL,
+           s->peak_used * 4ULL);
   return D3D_OK;
 }
 
@@ -667,10 +898,20 @@ int d3d_server_destroy(d3d_server s) {
   if (!s) return D3D_OK;
   for (cudaStream_t l : s->lane)
     if (l) cudaStreamSynchronize(l);
+  if (s->res_stream) cudaStreamSynchronize(s->res_stream);
   if (s->copy) cudaStreamSynchronize(s->copy);
   for (Request* r : s->queued) delete r;
   for (Request* r : s->active) free_request(s, r);
+  for (Request* r : s->res_pending) free_request(s, r);
   for (Request* r : s->retiring) free_request(s, r);
+  for (ResStaging& st : s->rstage) {
+    if (st.h) cudaFreeHost(st.h);
+    if (st.d) cudaFree(st.d);
+    if (st.d_steps) cudaFree(st.d_steps);
+    if (st.d_queue) cudaFree(st.d_queue);
+    if (st.done) cudaEventDestroy(st.done);
+  }
+  if (s->res_stream) cudaStreamDestroy(s->res_stream);
   for (auto& st : s->stage) {
     if (st.h_desc) cudaFreeHost(st.h_desc);
     if (st.h_items) cudaFreeHost(st.h_items);

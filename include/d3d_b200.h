@@ -369,6 +369,15 @@ int d3d_server_set_kernel(d3d_server server, int kernel);
  * for one another, so one stream's launch tail overlaps another's work. */
 int d3d_server_set_lanes(d3d_server server, int lanes);
 
+/* Whether an idle server (D3D_E_BUSY otherwise) runs the solves that fit
+ * the cluster-resident kernel on it (default on): such a solve (its grid
+ * within one cluster's shared memory, the rule of D3D_BATCH_KIND_RESIDENT)
+ * takes one dense buffer of the arena instead of two, and all of its steps
+ * run in one persistent launch per cluster size together with the other
+ * such solves admitted in the same tick; the ticks' step launches carry
+ * only the larger solves. */
+int d3d_server_set_resident(d3d_server server, int on);
+
 /* Number of requests queued, active on the device and copying out. */
 int d3d_server_pending(d3d_server server, int* queued, int* active,
                        int* retiring);

@@ -26,8 +26,8 @@ def _requests(seed, n, max_side=48, max_steps=40, cubic=False):
 
 
 def _serve(reqs, arena_bytes=1 << 28, chunk=8, interleave=False,
-           kernel=None, lanes=None):
-    server = B.Server(arena_bytes, chunk, kernel, lanes)
+           kernel=None, lanes=None, resident=None):
+    server = B.Server(arena_bytes, chunk, kernel, lanes, resident)
     outs = [np.full_like(f, np.nan) for f, _, _ in reqs]
     ids = {}
     done = set()
@@ -77,8 +77,9 @@ def test_every_step_kernel_bit_exact(kernel, lanes):
         f = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), 70 + i)
         reqs.append((f, (i * 7) % 13, c))
     outs, stats = _serve(reqs, chunk=5, interleave=True, kernel=kernel,
-                         lanes=lanes)
+                         lanes=lanes, resident=False)
     assert stats["kernel"] == kernel and stats["lanes"] == lanes
+    assert stats["resident_solves"] == 0
     for (f, steps, c), o in zip(reqs, outs):
         assert o.tobytes() == O.run(f, c, steps).tobytes()
     assert B.check_device_errors() == 0
@@ -103,6 +104,8 @@ def test_kernel_and_lanes_change_only_when_idle():
             server.set_lanes(bad)
     with pytest.raises(B.D3DError):
         server.set_kernel(7)
+    server.set_resident(False)
+    server.set_resident(True)
     server.close()
 
 
@@ -143,13 +146,57 @@ def test_small_arena_queues_until_space_frees():
 
 
 def test_rejects_solves_that_can_never_fit():
-    server = B.Server(1 << 20)
+    server = B.Server(1 << 20, resident=False)
     f = np.zeros((64, 64, 64), np.float32)  # 2 x 1 MiB > 1 MiB arena
     o = np.zeros_like(f)
     with pytest.raises(B.D3DError) as ei:
         server.submit(f, o, 3, O.params(64, 64, 64)[0])
     assert ei.value.code == B.D3D_E_BUSY
     server.close()
+    # On the cluster-resident path the same solve needs one buffer only.
+    server = B.Server(1 << 20)
+    f = O.seeded_noise((64, 64, 64), 3, amplitude=1.0)
+    server.submit(f, o, 3, O.params(64, 64, 64)[0])
+    server.drain()
+    assert o.tobytes() == O.run(f, O.params(64, 64, 64)[0], 3).tobytes()
+    assert server.stats()["resident_solves"] == 1
+    f = np.zeros((64, 64, 65), np.float32)  # 1 MiB + 16 KiB: never fits
+    o = np.zeros_like(f)
+    with pytest.raises(B.D3DError) as ei:
+        server.submit(f, o, 3, O.params(65, 64, 64)[0])
+    assert ei.value.code == B.D3D_E_BUSY
+    server.close()
+
+
+@pytest.mark.parametrize("lanes", [1, 4])
+def test_resident_path_matches_the_tick_path(lanes):
+    """Solves the cluster-resident kernel fits (all its cluster sizes,
+    every pad count, single planes and rows) and larger ones beside them:
+    every result equals the oracle's with the resident path on and off,
+    alone and interleaved with later arrivals."""
+    dims = [(1, 1, 1), (5, 3, 2), (17, 23, 5), (64, 64, 64), (88, 80, 37),
+            (96, 96, 80), (95, 7, 300), (33, 60, 45), (130, 80, 30),
+            (96, 96, 96), (250, 40, 9), (40, 40, 200)]
+    reqs = []
+    for i, (nx, ny, nz) in enumerate(dims):
+        c = B.batch_coefficients(nx, ny, nz, 0.05 + 0.01 * i)
+        f = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), 90 + i)
+        reqs.append((f, 1 + (i * 5) % 17, c))
+    on, st_on = _serve(reqs, arena_bytes=1 << 30, chunk=4, interleave=True,
+                       lanes=lanes)
+    off, st_off = _serve(reqs, arena_bytes=1 << 30, chunk=4,
+                         interleave=True, lanes=lanes, resident=False)
+    for (f, steps, c), a, b in zip(reqs, on, off):
+        ref = O.run(f, c, steps)
+        assert a.tobytes() == ref.tobytes()
+        assert b.tobytes() == ref.tobytes()
+    # (96, 96, 96) needs 20 CTAs; (130, 80, 30) and (250, 40, 9) have more
+    # than 2304 row segments a plane: those three run on the ticks
+    assert st_on["resident_solves"] == len(reqs) - 3
+    assert st_off["resident_solves"] == 0
+    alone, _ = _serve([reqs[5]], arena_bytes=1 << 30)
+    assert alone[0].tobytes() == on[5].tobytes()
+    assert B.check_device_errors() == 0
 
 
 def test_zero_step_requests_return_their_input():
