@@ -131,7 +131,10 @@ def test_standalone_driver_prints_reference_known_answers(kernel):
 
 @pytest.mark.gpu
 @pytest.mark.skipif(not os.path.exists(DROPIN),
-                    reason="drop-in build not present")
+                    reason="the drop-in driver links the reference's own "
+                           "objects, so it is built (oracle/Makefile dropin) "
+                           "only where the reference tree is present, and "
+                           "this machine has no build of it")
 def test_dropin_driver_prints_reference_known_answers():
     acc, _ = _run_driver(DROPIN, "--size", "64", "--count", "100")
     assert acc == "7.976817e-06"
