@@ -750,8 +750,12 @@ def main():
                          "(tma, generic, tb2, tb3, tb4, step2d; f64_ "
                          "prefix for FP64) on a --side^3 field (side^2 for "
                          "step2d) of seeded uniform values and exit: a "
-                         "fixed small case to profile")
+                         "fixed small case to profile; `resident` runs a "
+                         "batch of --grids such grids on the cluster-"
+                         "resident kernel")
     ap.add_argument("--side", type=int, default=512)
+    ap.add_argument("--grids", type=int, default=128,
+                    help="with --only-kernel resident: grids in the batch")
     ap.add_argument("--count", type=int, default=4)
     ap.add_argument("--variant", type=int, default=None)
     ap.add_argument("--zchunk", type=int, default=0)
@@ -771,6 +775,8 @@ def run_one_kernel(args):
     """`args.count` steps of one kernel on a seeded field, then exit."""
     import torch
     import benchmarks_b200 as B
+    if args.only_kernel == "resident":
+        return run_resident_case(args)
     kernels = {"tma": (B.KERNEL_TMA, 1), "generic": (B.KERNEL_GENERIC, 1),
                "tb2": (B.KERNEL_TB, 2), "tb3": (B.KERNEL_TB, 3),
                "tb4": (B.KERNEL_TB, 4), "step2d": (B.KERNEL_AUTO, 1)}
@@ -795,6 +801,34 @@ def run_one_kernel(args):
     print("kernel case done: %s n=%d (%dD) x %d steps, %s, device flags %d"
           % (args.only_kernel, n, plan.ndim, args.count,
              plan.info()["last_kernel"], flags), flush=True)
+    return 1 if flags else 0
+
+
+def run_resident_case(args):
+    """A batch of `args.grids` cubic grids of side `args.side`, `args.count`
+    steps each, on the cluster-resident kernel (one class: one persistent
+    launch per run), run twice; prints the device time of the second run."""
+    import torch
+    import benchmarks_b200 as B
+    torch.cuda.set_device(0)
+    n = args.side
+    c = B.batch_coefficients(n, n, n, 0.1)
+    batch = B.Batch([(n, n, n, args.count, c)] * args.grids)
+    batch.set_kind(B.BATCH_KIND_RESIDENT)
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    batch.arena.uniform_(0.0, 1.0, generator=gen)
+    batch.run()
+    ms = batch.run()
+    info = batch.info()
+    flags = B.check_device_errors()
+    upd = float(n) ** 3 * args.count * args.grids
+    print(json.dumps({"case": "resident", "grids": args.grids, "side": n,
+                      "steps": args.count, "ms": ms,
+                      "gpts": upd / (ms / 1e3) / 1e9,
+                      "resident": info["resident"],
+                      "launches_per_run": info["launches_per_run"],
+                      "device_flags": flags}), flush=True)
+    batch.close()
     return 1 if flags else 0
 
 
