@@ -772,7 +772,7 @@ int d3d_batch_autotune(d3d_batch b, void* stream) {
     if (probe_steps == 0) continue;
     float best = -1.0f;
     int best_kind = c.kind;
-    for (int kind = 0; kind < kNumKinds; ++kind) {
+    for (int kind = 0; kind < kResidentKind; ++kind) {  // per-class kinds
       if (kind_nr(kind) && !b->pitched) continue;
       if (kind_two(kind) && !class_takes_two_step(b, c)) continue;
       c.kind = kind;

@@ -21,7 +21,10 @@
 //      memory into registers, and the plane above its slab (the t of its
 //      last plane) into a one-plane halo buffer of its own CTA (DSMEM loads,
 //      ld.shared::cluster; no TMA, no multicast);
-//   3. cluster barrier: every pull is done, so planes may be overwritten;
+//   3. cluster barrier: every pull is done, so planes may be overwritten
+//      (each thread arrives right after its pulls and waits only before
+//      its first write, so the new values of the first plane are computed
+//      while the other CTAs arrive);
 //   4. z-march over the slab, in place: b and c of each thread's 16-byte
 //      segments ride in registers, t, n, s come from shared memory, x
 //      neighbours from shuffles (lanes at a row or warp edge read the
@@ -46,14 +49,20 @@ namespace d3d {
 namespace {
 
 // Every thread of every CTA of the cluster arrives (release) and waits
-// (acquire): shared-memory writes before it, local or remote, are visible
-// to every thread of the cluster after it.  The non-.aligned forms, so a
-// warp need not be converged when it reaches the barrier.
+// (acquire): shared-memory accesses before the arrive, local or remote, are
+// ordered before every access of the cluster after the wait.  The
+// non-.aligned forms, so a warp need not be converged at the barrier.  A
+// thread alternates arrive and wait; work between the two overlaps the
+// other CTAs' arrival.
+__device__ __forceinline__ void cluster_arrive() {
+  asm volatile("barrier.cluster.arrive.release;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() {
+  asm volatile("barrier.cluster.wait.acquire;" ::: "memory");
+}
 __device__ __forceinline__ void cluster_sync_all() {
-  asm volatile(
-      "barrier.cluster.arrive.release;\n\t"
-      "barrier.cluster.wait.acquire;" ::
-          : "memory");
+  cluster_arrive();
+  cluster_wait();
 }
 
 __device__ __forceinline__ unsigned cluster_rank() {
@@ -169,8 +178,9 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
   const uint32_t above = z1 < nz ? map_to_rank(sm_base, rank + 1) : 0u;
 
   V16<float> bq[UMAX], cq[UMAX], nv[UMAX];
+  cluster_arrive();  // the slab is loaded
   for (int s = 0; s < d.steps; ++s) {
-    cluster_sync_all();  // planes of the previous step complete everywhere
+    cluster_wait();  // planes of the previous step complete everywhere
     if (np > 0) {
 #pragma unroll
       for (int i = 0; i < UMAX; ++i) {
@@ -180,7 +190,9 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
           st16_shared(halo + c_off[i], ld16_cluster(above + 4u * c_off[i]));
       }
     }
-    cluster_sync_all();  // every pull done: planes may be overwritten
+    // This thread's pulls are done; the new values of plane 0 are computed
+    // before the wait, so the other CTAs' arrival overlaps that work.
+    cluster_arrive();
     if (np > 0) {
 #pragma unroll
       for (int i = 0; i < UMAX; ++i) cq[i] = ld16_shared(sm + c_off[i]);
@@ -214,15 +226,20 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
           bq[i] = c;
           cq[i] = t;
         }
-        __syncthreads();  // plane p read everywhere: overwrite it
+        __syncthreads();  // plane p read everywhere in this CTA
+        if (p == 0) cluster_wait();  // every pull of the cluster is done
 #pragma unroll
         for (int i = 0; i < UMAX; ++i)
           if (fl[i] & kValid) st16_shared(pl + c_off[i], nv[i]);
       }
+    } else {
+      cluster_wait();
     }
     if (rank == 0 && tid == 0)
       *reinterpret_cast<volatile int*>(steps_done + g) = s + 1;
+    cluster_arrive();  // this step's planes are written
   }
+  cluster_wait();
   __syncthreads();
   // Store the slab: the first nx floats of each row.
   {
