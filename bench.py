@@ -225,7 +225,8 @@ def batched_leg(B, torch, n_grids=4096, plain_sample=64, kind=None):
             "speedup_solves": solves / plain_solves}
 
 
-def serving_leg(B, torch, n_req=256, arena_gb=24.0, chunk=8):
+def serving_leg(B, torch, n_req=256, arena_gb=24.0, chunk=8, resident=None,
+                compare=True):
     """Config: Poisson stream (mean 2000 req/s) of cubic FP32 solves, sides
     log-uniform in [32, 256], steps log-uniform in [10, 2000]; the
     continuous-batching server vs a plain per-request loop (allocate,
@@ -260,7 +261,8 @@ def serving_leg(B, torch, n_req=256, arena_gb=24.0, chunk=8):
         return pool[offs[i]:offs[i] + s ** 3].reshape(s, s, s)
 
     def serve(out_pool, kernel=None, lanes=None):
-        server = B.Server(int(arena_gb * 2 ** 30), chunk, kernel, lanes)
+        server = B.Server(int(arena_gb * 2 ** 30), chunk, kernel, lanes,
+                          resident)
         done_at = [0.0] * n_req
         idmap = {}
         nxt = 0
@@ -291,6 +293,8 @@ def serving_leg(B, torch, n_req=256, arena_gb=24.0, chunk=8):
     # streams), then the same stream through the batch API's march kernel
     # on one stream for comparison
     served = serve(out_served)
+    if not compare:
+        return {"requests": n_req, "served": served}
     march = serve(out_other, kernel=-1, lanes=1)
     march_mismatched = same_results(out_served, out_other)
     # plain per-request loop
