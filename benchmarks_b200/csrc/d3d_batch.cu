@@ -463,25 +463,14 @@ int plan_resident(d3d_batch b) {
     cudaGetLastError();
     return D3D_OK;
   }
-  const size_t cap = d3d::kResidentSmemMax / 4;  // floats a CTA may hold
-  std::vector<std::pair<int, int>> keys;          // (cluster, variant)
+  std::vector<std::pair<int, int>> keys;  // (cluster, variant)
   for (int i = 0; i < n; ++i) {
     const d3d_batch_grid& g = b->grids[i];
     if (g.steps < 1) continue;
-    const int px = pitch_of(g.nx), segs = px / 4;
-    const long long plane = (long long)px * g.ny;
-    const long long units = (long long)segs * g.ny;
-    int v = -1;
-    for (int j = 0; j < d3d::kNumResidentVariants && v < 0; ++j) {
-      const d3d::ResidentVariant& rv = d3d::resident_variant(j);
-      if (units <= (long long)rv.threads * rv.units) v = j;
-    }
-    if (v < 0) continue;
-    const long long pmax = (long long)cap / plane - 1;
-    if (pmax < 1) continue;
-    const int cl = (int)((g.nz + pmax - 1) / pmax);
-    if (cl > d3d::kResidentMaxCluster) continue;
-    const int pc = (g.nz + cl - 1) / cl;
+    d3d::ResidentFit fit;
+    if (!d3d::resident_fit(g.nx, g.ny, g.nz, &fit)) continue;
+    const int px = fit.px, segs = px / 4, cl = fit.cluster, v = fit.variant;
+    const int pc = fit.pc;
     d3d::ResidentDesc& d = b->rdesc[i];
     d.in = b->arena + g.offset_a;
     d.out = b->arena + ((g.steps & 1) ? g.offset_b : g.offset_a);
@@ -508,7 +497,7 @@ int plan_resident(d3d_batch b) {
     }
     ResidentClass& rc = b->rclasses[ci];
     rc.grids.push_back(i);
-    rc.smem = std::max(rc.smem, (size_t)((pc + 1) * plane * 4));
+    rc.smem = std::max(rc.smem, fit.smem);
     b->rclass_of[i] = ci;
     b->resident_ok[i] = 1;
   }

@@ -234,6 +234,17 @@ constexpr int kResidentMaxCluster = 16;
 // Dynamic shared memory a CTA may hold: its pc planes and a halo plane.
 constexpr size_t kResidentSmemMax = 232448 - 1024;
 const ResidentVariant& resident_variant(int v);
+// Launch class of one grid on the resident kernel: the smallest thread
+// shape that covers its ceil(nx/4) * ny row segments a plane, and the
+// fewest CTAs (<= 16) of pc planes plus a halo plane each that fit the
+// shared memory a CTA may take -- a share of the SM for the narrow shapes
+// (128 and 256 threads), so 512 threads run on an SM, unless that needs
+// more than 16 CTAs.  False: the grid does not fit.
+struct ResidentFit {
+  int cluster, variant, pc, px;
+  size_t smem;
+};
+bool resident_fit(int nx, int ny, int nz, ResidentFit* fit);
 // Opts the kernels into the full shared memory and 16-CTA clusters on the
 // current device (once per device).
 cudaError_t resident_prepare();

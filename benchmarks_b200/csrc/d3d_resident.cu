@@ -149,7 +149,12 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
 
   // This thread's units u = tid + i * NT of the plane (S segments a row).
   const int units = S * ny;
-  int c_off[UMAX];
+  // Narrow thread shapes (2 units a thread) keep the rows above and below
+  // as offsets and rotate three register sets through the b, c, t roles;
+  // the wide ones (4 and 6 units) derive the row offsets from the flags and
+  // move c and t down a role each plane, which needs one register set less.
+  constexpr bool kWide = UMAX > 2;
+  int c_off[UMAX], n_off[UMAX], s_off[UMAX];
   unsigned fl[UMAX];  // flag bits; bits 8..9: index of x = nx-1 if kCross
 #pragma unroll
   for (int i = 0; i < UMAX; ++i) {
@@ -159,6 +164,8 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
     const int y = uu / S, seg = uu - y * S;
     const int xg = 4 * seg;
     c_off[i] = y * px + xg;
+    n_off[i] = y == 0 ? c_off[i] : c_off[i] - px;        // y = 0: own row
+    s_off[i] = y == ny - 1 ? c_off[i] : c_off[i] + px;   // y = ny-1: own row
     unsigned f = valid ? kValid : 0u;
     if (seg == 0) f |= kWOwn;
     else if (lane == 0) f |= kWSm;
@@ -177,14 +184,53 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
       z0 > 0 ? map_to_rank(sm_base, rank - 1) + 4u * (pc - 1) * plane : 0u;
   const uint32_t above = z1 < nz ? map_to_rank(sm_base, rank + 1) : 0u;
 
-  V16<float> bq[UMAX], cq[UMAX], nv[UMAX];
+  // One plane of the march: b in vb, c in vc, t loaded into vt (three
+  // register sets whose roles rotate, so nothing is copied), the new values
+  // held until every thread of the CTA has read plane p, then stored over
+  // it.  Before the first store of a step, every CTA's pulls must be done.
+  V16<float> q0[UMAX], q1[UMAX], q2[UMAX], nv[UMAX];
+  auto plane_step = [&](int p, const V16<float>* vb, const V16<float>* vc,
+                        V16<float>* vt) {
+    float* pl = sm + p * plane;
+    const float* tp = p + 1 < np ? pl + plane : (z1 < nz ? halo : pl);
+#pragma unroll
+    for (int i = 0; i < UMAX; ++i) {
+      const unsigned f = fl[i];
+      const V16<float> c = vc[i];
+      vt[i] = ld16_shared(tp + c_off[i]);
+      const int no = kWide ? c_off[i] - ((f & kNOwn) ? 0 : px) : n_off[i];
+      const int sof = kWide ? c_off[i] + ((f & kSOwn) ? 0 : px) : s_off[i];
+      const V16<float> n = ld16_shared(pl + no);
+      const V16<float> so = ld16_shared(pl + sof);
+      float wl = __shfl_up_sync(0xffffffffu, c.e[3], 1);
+      float er = __shfl_down_sync(0xffffffffu, c.e[0], 1);
+      wl = ld_shared_if(f & kWSm, pl + c_off[i] - 1, wl);
+      if (f & kWOwn) wl = c.e[0];
+      er = ld_shared_if(f & kESm, pl + c_off[i] + 4, er);
+      if (f & kEOwn) er = c.e[3];
+      V16<float> o = point_seg<float>(kk, c, n, so, vb[i], vt[i], wl, er);
+      if (f & kCross) {
+        const unsigned jh = (f >> 8) & 3u;
+        if (jh < 1) o.e[1] = o.e[0];
+        if (jh < 2) o.e[2] = o.e[1];
+        o.e[3] = o.e[2];
+      }
+      nv[i] = o;
+    }
+    __syncthreads();  // plane p read everywhere in this CTA
+    if (p == 0) cluster_wait();  // every pull of the cluster is done
+#pragma unroll
+    for (int i = 0; i < UMAX; ++i)
+      if (fl[i] & kValid) st16_shared(pl + c_off[i], nv[i]);
+  };
+
   cluster_arrive();  // the slab is loaded
   for (int s = 0; s < d.steps; ++s) {
     cluster_wait();  // planes of the previous step complete everywhere
     if (np > 0) {
 #pragma unroll
       for (int i = 0; i < UMAX; ++i) {
-        bq[i] = z0 > 0 ? ld16_cluster(below + 4u * c_off[i])
+        q0[i] = z0 > 0 ? ld16_cluster(below + 4u * c_off[i])
                        : ld16_shared(sm + c_off[i]);
         if (z1 < nz && (fl[i] & kValid))
           st16_shared(halo + c_off[i], ld16_cluster(above + 4u * c_off[i]));
@@ -195,42 +241,24 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
     cluster_arrive();
     if (np > 0) {
 #pragma unroll
-      for (int i = 0; i < UMAX; ++i) cq[i] = ld16_shared(sm + c_off[i]);
-      for (int p = 0; p < np; ++p) {
-        float* pl = sm + p * plane;
-        const float* tp =
-            p + 1 < np ? pl + plane : (z1 < nz ? halo : pl);
+      for (int i = 0; i < UMAX; ++i) q1[i] = ld16_shared(sm + c_off[i]);
+      if constexpr (kWide) {
+        for (int p = 0; p < np; ++p) {
+          plane_step(p, q0, q1, q2);
 #pragma unroll
-        for (int i = 0; i < UMAX; ++i) {
-          const unsigned f = fl[i];
-          const V16<float> c = cq[i];
-          const V16<float> t = ld16_shared(tp + c_off[i]);
-          const V16<float> n =
-              ld16_shared(pl + c_off[i] - ((f & kNOwn) ? 0 : px));
-          const V16<float> so =
-              ld16_shared(pl + c_off[i] + ((f & kSOwn) ? 0 : px));
-          float wl = __shfl_up_sync(0xffffffffu, c.e[3], 1);
-          float er = __shfl_down_sync(0xffffffffu, c.e[0], 1);
-          wl = ld_shared_if(f & kWSm, pl + c_off[i] - 1, wl);
-          if (f & kWOwn) wl = c.e[0];
-          er = ld_shared_if(f & kESm, pl + c_off[i] + 4, er);
-          if (f & kEOwn) er = c.e[3];
-          V16<float> o = point_seg<float>(kk, c, n, so, bq[i], t, wl, er);
-          if (f & kCross) {
-            const unsigned jh = (f >> 8) & 3u;
-            if (jh < 1) o.e[1] = o.e[0];
-            if (jh < 2) o.e[2] = o.e[1];
-            o.e[3] = o.e[2];
+          for (int i = 0; i < UMAX; ++i) {
+            q0[i] = q1[i];
+            q1[i] = q2[i];
           }
-          nv[i] = o;
-          bq[i] = c;
-          cq[i] = t;
         }
-        __syncthreads();  // plane p read everywhere in this CTA
-        if (p == 0) cluster_wait();  // every pull of the cluster is done
-#pragma unroll
-        for (int i = 0; i < UMAX; ++i)
-          if (fl[i] & kValid) st16_shared(pl + c_off[i], nv[i]);
+      } else {
+        for (int p = 0; p < np; p += 3) {
+          plane_step(p, q0, q1, q2);
+          if (p + 1 >= np) break;
+          plane_step(p + 1, q1, q2, q0);
+          if (p + 2 >= np) break;
+          plane_step(p + 2, q2, q0, q1);
+        }
       }
     } else {
       cluster_wait();
@@ -253,8 +281,10 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
   }
 }
 
+// The narrow shapes run several CTAs an SM (512 threads in all): their
+// registers are capped to fit.
 template <int NT, int UMAX>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, (NT < 512 ? 512 / NT : 1))
     resident_kernel(const ResidentDesc* __restrict__ descs, int ngrids,
                     unsigned* __restrict__ queue,
                     int* __restrict__ steps_done) {
@@ -338,6 +368,36 @@ __global__ void set_counters_kernel(const int2* __restrict__ id_steps, int n,
 }  // namespace
 
 const ResidentVariant& resident_variant(int v) { return kResident[v]; }
+
+bool resident_fit(int nx, int ny, int nz, ResidentFit* fit) {
+  const int px = (nx + 3) / 4 * 4, segs = px / 4;
+  const long long plane = (long long)px * ny;
+  const long long units = (long long)segs * ny;
+  int v = -1;
+  for (int j = 0; j < kNumResidentVariants && v < 0; ++j)
+    if (units <= (long long)kResident[j].threads * kResident[j].units) v = j;
+  if (v < 0) return false;
+  // Shared memory a CTA may take so that 512 threads share an SM (several
+  // CTAs of the narrow shapes: their barrier waits overlap each other's
+  // work); the whole allowance if the grid needs more than 16 CTAs then.
+  const int per_sm = std::max(1, 512 / kResident[v].threads);
+  const size_t caps[2] = {
+      std::min(kResidentSmemMax, (size_t)(233472 / per_sm) - 1024),
+      kResidentSmemMax};
+  for (size_t cap : caps) {
+    const long long pmax = (long long)(cap / 4) / plane - 1;
+    if (pmax < 1) continue;
+    const int cl = (int)((nz + pmax - 1) / pmax);
+    if (cl > kResidentMaxCluster) continue;
+    fit->cluster = cl;
+    fit->variant = v;
+    fit->pc = (nz + cl - 1) / cl;
+    fit->smem = (size_t)((fit->pc + 1) * plane * 4);
+    fit->px = px;
+    return true;
+  }
+  return false;
+}
 
 cudaError_t launch_set_counters(const int2* id_steps, int n, int* counters,
                                 cudaStream_t s) {

@@ -253,21 +253,10 @@ void plan_resident_solve(d3d_server s, Request* r) {
     s->resident = false;
     return;
   }
-  const int px = (r->nx + 3) / 4 * 4, segs = px / 4;
-  const long long plane = (long long)px * r->ny;
-  const long long units = (long long)segs * r->ny;
-  int v = -1;
-  for (int j = 0; j < d3d::kNumResidentVariants && v < 0; ++j) {
-    const d3d::ResidentVariant& rv = d3d::resident_variant(j);
-    if (units <= (long long)rv.threads * rv.units) v = j;
-  }
-  if (v < 0) return;
-  const long long pmax = (long long)(d3d::kResidentSmemMax / 4) / plane - 1;
-  if (pmax < 1) return;
-  const int cl = (int)((r->nz + pmax - 1) / pmax);
-  if (cl > d3d::kResidentMaxCluster) return;
-  const int pc = (r->nz + cl - 1) / cl;
-  const size_t smem = (size_t)((pc + 1) * plane * 4);
+  d3d::ResidentFit fit;
+  if (!d3d::resident_fit(r->nx, r->ny, r->nz, &fit)) return;
+  const int cl = fit.cluster, v = fit.variant, pc = fit.pc;
+  const size_t smem = fit.smem;
   if (res_max_clusters(s, v, cl, smem) < 1) return;
   r->resident = true;
   r->r_cluster = cl;
