@@ -180,8 +180,10 @@ struct d3d_server_s {
   bool resident = true;
   std::vector<Request*> res_pending;
   cudaStream_t res_stream = nullptr;
-  ResStaging rstage[2];
-  int res_index = 0;
+  // Group stagings: one is reused only once its launches have ended (an
+  // event query, never a host wait), so a long small solve does not hold
+  // up the ticks; a new one is made when none is free.
+  std::vector<ResStaging*> rstage;
   long long res_solves = 0, res_launches = 0;
   std::map<std::tuple<int, int, size_t>, int> res_max_clusters;
 };
@@ -400,11 +402,23 @@ int admit(d3d_server s) {
 // result is copied out once the group's launches end.
 int launch_resident_group(d3d_server s) {
   if (s->res_pending.empty()) return D3D_OK;
-  ResStaging& st = s->rstage[s->res_index & 1];
-  if (st.in_flight) {
-    S_TRY(cudaEventSynchronize(st.done), "cudaEventSynchronize");
-    st.in_flight = false;
+  ResStaging* free_st = nullptr;
+  for (ResStaging* c : s->rstage) {
+    if (c->in_flight) {
+      const cudaError_t q = cudaEventQuery(c->done);
+      if (q == cudaErrorNotReady) continue;
+      if (q != cudaSuccess) return d3d::set_cuda_error(q, "resident group");
+      c->in_flight = false;
+    }
+    free_st = c;
+    break;
   }
+  if (!free_st) {
+    free_st = new (std::nothrow) ResStaging();
+    if (!free_st) return sfail(D3D_E_OOM, "resident staging");
+    s->rstage.push_back(free_st);
+  }
+  ResStaging& st = *free_st;
   std::vector<Request*>& list = s->res_pending;
   std::stable_sort(list.begin(), list.end(), [](const Request* x,
                                                 const Request* y) {
@@ -421,7 +435,7 @@ int launch_resident_group(d3d_server s) {
     st.h = nullptr;
     st.d = nullptr;
     st.d_steps = nullptr;
-    st.cap = std::max(n, 2 * st.cap);
+    st.cap = std::max({n, 2 * st.cap, (size_t)256});
     S_TRY(cudaMallocHost(&st.h, st.cap * sizeof(d3d::ResidentDesc)),
           "cudaMallocHost (resident staging)");
     S_TRY(cudaMalloc(&st.d, st.cap * sizeof(d3d::ResidentDesc)),
@@ -482,7 +496,6 @@ int launch_resident_group(d3d_server s) {
   }
   S_TRY(cudaEventRecord(st.done, rs), "cudaEventRecord");
   st.in_flight = true;
-  ++s->res_index;
   S_TRY(cudaStreamWaitEvent(s->copy, st.done, 0), "cudaStreamWaitEvent");
   for (Request* r : list) {
     S_TRY(cudaMemcpyAsync(r->host_out, s->arena + r->off_a, dense_bytes(r),
@@ -893,12 +906,13 @@ int d3d_server_destroy(d3d_server s) {
   for (Request* r : s->active) free_request(s, r);
   for (Request* r : s->res_pending) free_request(s, r);
   for (Request* r : s->retiring) free_request(s, r);
-  for (ResStaging& st : s->rstage) {
-    if (st.h) cudaFreeHost(st.h);
-    if (st.d) cudaFree(st.d);
-    if (st.d_steps) cudaFree(st.d_steps);
-    if (st.d_queue) cudaFree(st.d_queue);
-    if (st.done) cudaEventDestroy(st.done);
+  for (ResStaging* st : s->rstage) {
+    if (st->h) cudaFreeHost(st->h);
+    if (st->d) cudaFree(st->d);
+    if (st->d_steps) cudaFree(st->d_steps);
+    if (st->d_queue) cudaFree(st->d_queue);
+    if (st->done) cudaEventDestroy(st->done);
+    delete st;
   }
   if (s->res_stream) cudaStreamDestroy(s->res_stream);
   for (auto& st : s->stage) {
