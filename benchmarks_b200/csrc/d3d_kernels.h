@@ -229,17 +229,17 @@ struct ResidentDesc {
 struct ResidentVariant {
   int threads, units;
 };
-constexpr int kNumResidentVariants = 5;
+constexpr int kNumResidentVariants = 6;
 constexpr int kResidentMaxCluster = 16;
 // Dynamic shared memory a CTA may hold: its pc planes and a halo plane.
 constexpr size_t kResidentSmemMax = 232448 - 1024;
 const ResidentVariant& resident_variant(int v);
-// Launch class of one grid on the resident kernel: the smallest thread
-// shape that covers its ceil(nx/4) * ny row segments a plane, and the
-// fewest CTAs (<= 16) of pc planes plus a halo plane each that fit the
-// shared memory a CTA may take -- a share of the SM for the narrow shapes
-// (128 and 256 threads), so 512 threads run on an SM, unless that needs
-// more than 16 CTAs.  False: the grid does not fit.
+// Launch class of one grid on the resident kernel: the narrowest thread
+// shape that covers its ceil(nx/4) * ny row segments a plane and holds the
+// grid in at most 16 CTAs of pc planes plus a halo plane each, within the
+// shared memory a CTA of that shape may take -- a share of the SM for the
+// 128- and 256-thread shapes, so that 512 threads run on an SM.  False: no
+// shape fits the grid.
 struct ResidentFit {
   int cluster, variant, pc, px;
   size_t smem;

@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(NT, (NT < 512 ? 512 / NT : 1))
 // (threads, units a thread at most): a plane of S * ny 16-byte segments
 // fits variant v when S * ny <= threads * units.
 const ResidentVariant kResident[kNumResidentVariants] = {
-    {128, 2}, {256, 2}, {512, 2}, {512, 4}, {384, 6}};
+    {128, 2}, {256, 2}, {256, 4}, {512, 2}, {512, 4}, {384, 6}};
 
 template <int NT, int UMAX>
 cudaError_t launch_v(const ResidentDesc* descs, int ngrids, unsigned* queue,
@@ -373,18 +373,18 @@ bool resident_fit(int nx, int ny, int nz, ResidentFit* fit) {
   const int px = (nx + 3) / 4 * 4, segs = px / 4;
   const long long plane = (long long)px * ny;
   const long long units = (long long)segs * ny;
-  int v = -1;
-  for (int j = 0; j < kNumResidentVariants && v < 0; ++j)
-    if (units <= (long long)kResident[j].threads * kResident[j].units) v = j;
-  if (v < 0) return false;
-  // Shared memory a CTA may take so that 512 threads share an SM (several
-  // CTAs of the narrow shapes: their barrier waits overlap each other's
-  // work); the whole allowance if the grid needs more than 16 CTAs then.
-  const int per_sm = std::max(1, 512 / kResident[v].threads);
-  const size_t caps[2] = {
-      std::min(kResidentSmemMax, (size_t)(233472 / per_sm) - 1024),
-      kResidentSmemMax};
-  for (size_t cap : caps) {
+  // Thread shapes in order of preference, narrowest first: a narrow shape
+  // takes a share of the SM's shared memory so that 512 threads (several
+  // CTAs of different clusters) run on an SM and one CTA's barrier waits
+  // overlap another's work.  The first shape that covers the plane and
+  // needs at most 16 CTAs at its share wins; the 512- and 384-thread shapes
+  // take a whole SM.
+  for (int v = 0; v < kNumResidentVariants; ++v) {
+    const ResidentVariant& rv = kResident[v];
+    if (units > (long long)rv.threads * rv.units) continue;
+    const int per_sm = std::max(1, 512 / rv.threads);
+    const size_t cap =
+        std::min(kResidentSmemMax, (size_t)(233472 / per_sm) - 1024);
     const long long pmax = (long long)(cap / 4) / plane - 1;
     if (pmax < 1) continue;
     const int cl = (int)((nz + pmax - 1) / pmax);
@@ -415,6 +415,7 @@ cudaError_t resident_prepare() {
   if (done_dev == dev) return cudaSuccess;
   if ((e = prepare_v<128, 2>()) != cudaSuccess) return e;
   if ((e = prepare_v<256, 2>()) != cudaSuccess) return e;
+  if ((e = prepare_v<256, 4>()) != cudaSuccess) return e;
   if ((e = prepare_v<512, 2>()) != cudaSuccess) return e;
   if ((e = prepare_v<512, 4>()) != cudaSuccess) return e;
   if ((e = prepare_v<384, 6>()) != cudaSuccess) return e;
@@ -428,9 +429,10 @@ cudaError_t resident_max_clusters(int variant, int cluster, size_t smem,
   switch (variant) {
     case 0: return max_clusters_v<128, 2>(cluster, smem, out);
     case 1: return max_clusters_v<256, 2>(cluster, smem, out);
-    case 2: return max_clusters_v<512, 2>(cluster, smem, out);
-    case 3: return max_clusters_v<512, 4>(cluster, smem, out);
-    case 4: return max_clusters_v<384, 6>(cluster, smem, out);
+    case 2: return max_clusters_v<256, 4>(cluster, smem, out);
+    case 3: return max_clusters_v<512, 2>(cluster, smem, out);
+    case 4: return max_clusters_v<512, 4>(cluster, smem, out);
+    case 5: return max_clusters_v<384, 6>(cluster, smem, out);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -446,9 +448,10 @@ cudaError_t launch_resident(int variant, const ResidentDesc* descs,
   switch (variant) {
     case 0: return launch_v<128, 2>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
     case 1: return launch_v<256, 2>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
-    case 2: return launch_v<512, 2>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
-    case 3: return launch_v<512, 4>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
-    case 4: return launch_v<384, 6>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case 2: return launch_v<256, 4>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case 3: return launch_v<512, 2>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case 4: return launch_v<512, 4>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case 5: return launch_v<384, 6>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
     default: return cudaErrorInvalidValue;
   }
 }

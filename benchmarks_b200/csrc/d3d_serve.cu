@@ -496,14 +496,16 @@ int launch_resident_group(d3d_server s) {
   }
   S_TRY(cudaEventRecord(st.done, rs), "cudaEventRecord");
   st.in_flight = true;
-  S_TRY(cudaStreamWaitEvent(s->copy, st.done, 0), "cudaStreamWaitEvent");
+  // The results go out on the resident stream itself: the shared copy
+  // stream carries the inputs of later admissions, which must not wait for
+  // this group's launches.
   for (Request* r : list) {
     S_TRY(cudaMemcpyAsync(r->host_out, s->arena + r->off_a, dense_bytes(r),
-                          cudaMemcpyDeviceToHost, s->copy),
+                          cudaMemcpyDeviceToHost, rs),
           "D2H copy (result)");
     S_TRY(cudaEventCreateWithFlags(&r->ev_out, cudaEventDisableTiming),
           "cudaEventCreate");
-    S_TRY(cudaEventRecord(r->ev_out, s->copy), "cudaEventRecord");
+    S_TRY(cudaEventRecord(r->ev_out, rs), "cudaEventRecord");
     s->retiring.push_back(r);
     ++s->res_solves;
   }
