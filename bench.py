@@ -226,7 +226,7 @@ def batched_leg(B, torch, n_grids=4096, plain_sample=64, kind=None):
 
 
 def serving_leg(B, torch, n_req=256, arena_gb=24.0, chunk=8, resident=None,
-                compare=True):
+                compare=True, kernel=None):
     """Config: Poisson stream (mean 2000 req/s) of cubic FP32 solves, sides
     log-uniform in [32, 256], steps log-uniform in [10, 2000]; the
     continuous-batching server vs a plain per-request loop (allocate,
@@ -292,7 +292,7 @@ def serving_leg(B, torch, n_req=256, arena_gb=24.0, chunk=8, resident=None,
     # served: the default server (pitched TMA step kernel, several
     # streams), then the same stream through the batch API's march kernel
     # on one stream for comparison
-    served = serve(out_served)
+    served = serve(out_served, kernel=kernel)
     if not compare:
         return {"requests": n_req, "served": served}
     march = serve(out_other, kernel=-1, lanes=1)

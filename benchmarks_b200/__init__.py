@@ -572,7 +572,7 @@ class Server:
 
     def set_resident(self, on):
         """Whether the idle server runs the solves that fit it on the
-        cluster-resident kernel (default on)."""
+        cluster-resident kernel (default off)."""
         check(lib().d3d_server_set_resident(self._h, int(bool(on))))
 
     def pending(self):

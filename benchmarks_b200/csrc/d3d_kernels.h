@@ -229,7 +229,7 @@ struct ResidentDesc {
 struct ResidentVariant {
   int threads, units;
 };
-constexpr int kNumResidentVariants = 6;
+constexpr int kNumResidentVariants = 5;
 constexpr int kResidentMaxCluster = 16;
 // Dynamic shared memory a CTA may hold: its pc planes and a halo plane.
 constexpr size_t kResidentSmemMax = 232448 - 1024;

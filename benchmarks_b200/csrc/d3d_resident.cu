@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(NT, (NT < 512 ? 512 / NT : 1))
 // (threads, units a thread at most): a plane of S * ny 16-byte segments
 // fits variant v when S * ny <= threads * units.
 const ResidentVariant kResident[kNumResidentVariants] = {
-    {128, 2}, {256, 2}, {256, 4}, {512, 2}, {512, 4}, {384, 6}};
+    {128, 2}, {256, 2}, {512, 2}, {512, 4}, {384, 6}};
 
 template <int NT, int UMAX>
 cudaError_t launch_v(const ResidentDesc* descs, int ngrids, unsigned* queue,
@@ -378,7 +378,9 @@ bool resident_fit(int nx, int ny, int nz, ResidentFit* fit) {
   // CTAs of different clusters) run on an SM and one CTA's barrier waits
   // overlap another's work.  The first shape that covers the plane and
   // needs at most 16 CTAs at its share wins; the 512- and 384-thread shapes
-  // take a whole SM.
+  // take a whole SM.  (A 256-thread shape with 4 units a thread at half an
+  // SM measured 10-17% slower on B200 than 512 threads with 2 units at a
+  // whole SM, at 48^3 and 64^3.)
   for (int v = 0; v < kNumResidentVariants; ++v) {
     const ResidentVariant& rv = kResident[v];
     if (units > (long long)rv.threads * rv.units) continue;
@@ -415,7 +417,6 @@ cudaError_t resident_prepare() {
   if (done_dev == dev) return cudaSuccess;
   if ((e = prepare_v<128, 2>()) != cudaSuccess) return e;
   if ((e = prepare_v<256, 2>()) != cudaSuccess) return e;
-  if ((e = prepare_v<256, 4>()) != cudaSuccess) return e;
   if ((e = prepare_v<512, 2>()) != cudaSuccess) return e;
   if ((e = prepare_v<512, 4>()) != cudaSuccess) return e;
   if ((e = prepare_v<384, 6>()) != cudaSuccess) return e;
@@ -429,10 +430,9 @@ cudaError_t resident_max_clusters(int variant, int cluster, size_t smem,
   switch (variant) {
     case 0: return max_clusters_v<128, 2>(cluster, smem, out);
     case 1: return max_clusters_v<256, 2>(cluster, smem, out);
-    case 2: return max_clusters_v<256, 4>(cluster, smem, out);
-    case 3: return max_clusters_v<512, 2>(cluster, smem, out);
-    case 4: return max_clusters_v<512, 4>(cluster, smem, out);
-    case 5: return max_clusters_v<384, 6>(cluster, smem, out);
+    case 2: return max_clusters_v<512, 2>(cluster, smem, out);
+    case 3: return max_clusters_v<512, 4>(cluster, smem, out);
+    case 4: return max_clusters_v<384, 6>(cluster, smem, out);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -448,10 +448,9 @@ cudaError_t launch_resident(int variant, const ResidentDesc* descs,
   switch (variant) {
     case 0: return launch_v<128, 2>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
     case 1: return launch_v<256, 2>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
-    case 2: return launch_v<256, 4>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
-    case 3: return launch_v<512, 2>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
-    case 4: return launch_v<512, 4>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
-    case 5: return launch_v<384, 6>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case 2: return launch_v<512, 2>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case 3: return launch_v<512, 4>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case 4: return launch_v<384, 6>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
     default: return cudaErrorInvalidValue;
   }
 }

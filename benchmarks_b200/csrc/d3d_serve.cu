@@ -177,7 +177,7 @@ struct d3d_server_s {
   unsigned long long launches = 0, peak_used = 0;
   // Cluster-resident solves: admitted and waiting for the next group
   // launch; the stream and stagings of those launches.
-  bool resident = true;
+  bool resident = false;
   std::vector<Request*> res_pending;
   cudaStream_t res_stream = nullptr;
   // Group stagings: one is reused only once its launches have ended (an

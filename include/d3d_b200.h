@@ -370,7 +370,9 @@ int d3d_server_set_kernel(d3d_server server, int kernel);
 int d3d_server_set_lanes(d3d_server server, int lanes);
 
 /* Whether an idle server (D3D_E_BUSY otherwise) runs the solves that fit
- * the cluster-resident kernel on it (default on): such a solve (its grid
+ * the cluster-resident kernel on it (default off: on the 32..256 serving
+ * stream it measured slower, the resident launches taking whole SMs from
+ * the ticks' larger solves): such a solve (its grid
  * within one cluster's shared memory, the rule of D3D_BATCH_KIND_RESIDENT)
  * takes one dense buffer of the arena instead of two, and all of its steps
  * run in one persistent launch per cluster size together with the other

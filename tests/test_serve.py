@@ -154,7 +154,7 @@ def test_rejects_solves_that_can_never_fit():
     assert ei.value.code == B.D3D_E_BUSY
     server.close()
     # On the cluster-resident path the same solve needs one buffer only.
-    server = B.Server(1 << 20)
+    server = B.Server(1 << 20, resident=True)
     f = O.seeded_noise((64, 64, 64), 3, amplitude=1.0)
     server.submit(f, o, 3, O.params(64, 64, 64)[0])
     server.drain()
@@ -183,7 +183,7 @@ def test_resident_path_matches_the_tick_path(lanes):
         f = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), 90 + i)
         reqs.append((f, 1 + (i * 5) % 17, c))
     on, st_on = _serve(reqs, arena_bytes=1 << 30, chunk=4, interleave=True,
-                       lanes=lanes)
+                       lanes=lanes, resident=True)
     off, st_off = _serve(reqs, arena_bytes=1 << 30, chunk=4,
                          interleave=True, lanes=lanes, resident=False)
     for (f, steps, c), a, b in zip(reqs, on, off):
@@ -194,7 +194,7 @@ def test_resident_path_matches_the_tick_path(lanes):
     # than 2304 row segments a plane: those three run on the ticks
     assert st_on["resident_solves"] == len(reqs) - 3
     assert st_off["resident_solves"] == 0
-    alone, _ = _serve([reqs[5]], arena_bytes=1 << 30)
+    alone, _ = _serve([reqs[5]], arena_bytes=1 << 30, resident=True)
     assert alone[0].tobytes() == on[5].tobytes()
     assert B.check_device_errors() == 0
 
