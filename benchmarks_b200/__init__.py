@@ -82,6 +82,7 @@ _SIGNATURES = {
     "d3d_batch_progress": ([_vp, ctypes.POINTER(ctypes.c_int), _i], _i),
     "d3d_batch_destroy": ([_vp], _i),
     "d3d_server_set_resident": ([_vp, _i], _i),
+    "d3d_server_set_large_kernel": ([_vp, _i, _i], _i),
     "d3d_server_create": ([_sz, _i, _vpp], _i),
     "d3d_server_submit": ([_vp, _i, _i, _i, _i,
                            ctypes.POINTER(ctypes.c_float), _vp, _vp,
@@ -569,6 +570,13 @@ class Server:
     def set_lanes(self, lanes):
         """Compute streams of the idle server (1..4, default 4)."""
         check(lib().d3d_server_set_lanes(self._h, int(lanes)))
+
+    def set_large_kernel(self, kernel, min_px=128):
+        """Step kernel of the idle server's large solves (pitched rows of at
+        least min_px floats), on the upper half of the lanes; kernel < 0
+        turns it off."""
+        check(lib().d3d_server_set_large_kernel(self._h, int(kernel),
+                                                int(min_px)))
 
     def set_resident(self, on):
         """Whether the idle server runs the solves that fit it on the

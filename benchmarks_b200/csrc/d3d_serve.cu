@@ -48,6 +48,12 @@ int strip_nr(int kernel) {
   return kernel >= kStripBase ? kernel - kStripBase + 1 : 0;
 }
 constexpr int kMaxLanes = 4;               // compute streams
+// Step-kernel geometry of a kernel id: strip segments a thread (0 for the
+// tile forms and the march kernel) and, for the tile forms and the march
+// kernel, the xy tile.
+struct KernGeom {
+  int nr, bx, by;
+};
 constexpr int kDefaultLanes = 4;
 
 // First-fit allocator over the arena, in elements.
@@ -111,6 +117,7 @@ struct Request {
   int zc = 0, tiles = 0;  // this tick: planes per z slab, work items
   int n = 0;              // this tick: steps to run
   int lane = 0;           // compute stream that runs all its steps
+  int kern = 0;           // step kernel (the server's, or its large one)
   float coeff[7];
   const float* host_in;
   float* host_out;
@@ -160,6 +167,10 @@ struct d3d_server_s {
   ArenaAlloc alloc;
   int chunk = 8;
   int kernel = kDefaultKernel;  // pitched tile 0..4, strip 5..6, march -1
+  // Solves whose pitched rows are at least large_px floats use
+  // large_kernel (a pitched kernel) on the upper half of the lanes; the
+  // others use `kernel` on the lower half.  large_kernel < 0: off.
+  int large_kernel = -1, large_px = 0;
   std::deque<Request*> queued;
   std::vector<Request*> active;
   std::vector<Request*> retiring;
@@ -341,15 +352,19 @@ int admit(d3d_server s) {
     }
     r->off_a = a;
     r->off_b = b;
-    if (s->kernel >= 0) {
+    // (One lane runs one kernel: with a single lane there is no split.)
+    const bool large = s->kernel >= 0 && s->large_kernel >= 0 &&
+                       s->lanes > 1 && r->px >= s->large_px;
+    r->kern = large ? s->large_kernel : s->kernel;
+    if (r->kern >= 0) {
       int bxm, bym;
-      if (strip_nr(s->kernel)) {
-        r->strip = d3d::strip_shape(r->px, r->ny, strip_nr(s->kernel));
+      if (strip_nr(r->kern)) {
+        r->strip = d3d::strip_shape(r->px, r->ny, strip_nr(r->kern));
         bxm = 4 * r->strip.segs + 8;
         bym = r->strip.rows + 2;
       } else {
-        bxm = d3d::pitched_box_x(s->kernel);
-        bym = d3d::pitched_box_y(s->kernel);
+        bxm = d3d::pitched_box_x(r->kern);
+        bym = d3d::pitched_box_y(r->kern);
       }
       for (int m = 0; m < 2; ++m) {
         cudaError_t e = d3d::encode_field_map(
@@ -378,8 +393,16 @@ int admit(d3d_server s) {
     S_TRY(cudaEventCreateWithFlags(&r->ev_in, cudaEventDisableTiming),
           "cudaEventCreate");
     S_TRY(cudaEventRecord(r->ev_in, s->copy), "cudaEventRecord");
-    r->lane = 0;
-    for (int l = 1; l < s->lanes; ++l)
+    // With a large kernel, the two kernels keep to their own lanes.
+    int l0 = 0, l1 = s->lanes;
+    if (s->kernel >= 0 && s->large_kernel >= 0 && s->lanes > 1 &&
+        s->large_kernel != s->kernel) {
+      const int half = s->lanes / 2;
+      if (large) l0 = half;
+      else l1 = half;
+    }
+    r->lane = l0;
+    for (int l = l0 + 1; l < l1; ++l)
       if (work[l] < work[r->lane]) r->lane = l;
     work[r->lane] += (double)r->elems() * r->steps;
     S_TRY(cudaStreamWaitEvent(s->lane[r->lane], r->ev_in, 0),
@@ -575,20 +598,23 @@ int advance(d3d_server s) {
   }
   std::vector<Request*>& act = s->active;
   const bool pitched = s->kernel >= 0;
-  const int nr = strip_nr(s->kernel);
-  int bx = d3d::kBShapes[0].bx, by = d3d::kBShapes[0].by;
-  if (pitched && !nr) {
-    bx = 4 * d3d::pitched_variant(s->kernel).lanes;
-    by = d3d::pitched_variant(s->kernel).by;
-  }
+  auto geom = [](int kern) {
+    KernGeom g{strip_nr(kern), d3d::kBShapes[0].bx, d3d::kBShapes[0].by};
+    if (kern >= 0 && !g.nr) {
+      g.bx = 4 * d3d::pitched_variant(kern).lanes;
+      g.by = d3d::pitched_variant(kern).by;
+    }
+    return g;
+  };
   // xy work items of a solve: tiles_x across, tiles_xy in all.
   auto xy_tiles = [&](const Request* r, int* tx) {
-    if (nr) {
+    const KernGeom g = geom(r->kern);
+    if (g.nr) {
       *tx = r->strip.pieces;
       return r->strip.pieces * ((r->ny + r->strip.rows - 1) / r->strip.rows);
     }
-    *tx = (r->nx + bx - 1) / bx;
-    return *tx * ((r->ny + by - 1) / by);
+    *tx = (r->nx + g.bx - 1) / g.bx;
+    return *tx * ((r->ny + g.by - 1) / g.by);
   };
   size_t nitems = 0;
   for (int cap = kMaxSlab;; cap /= 2) {
@@ -701,6 +727,8 @@ int advance(d3d_server s) {
     // This lane's solves in launch order of their last step (they are
     // sorted by n, descending): retire each right after it.
     size_t fin = desc0[l + 1];
+    const int lk = act[desc0[l]]->kern;  // one kernel a lane
+    const int nr = strip_nr(lk);
     for (int j = 0; j < nj && act_l[j] > 0; ++j) {
       auto* pd = static_cast<d3d::PitchedDesc*>(st.d_desc);
       S_TRY(nr ? d3d::launch_pitched_strip(nr, pd, st.d_items + item0[l],
@@ -708,7 +736,7 @@ int advance(d3d_server s) {
                                            d3d::device_error_word())
             : pitched
                 ? d3d::launch_pitched_step(
-                      s->kernel, pd, st.d_items + item0[l], act_l[j], j & 1,
+                      lk, pd, st.d_items + item0[l], act_l[j], j & 1,
                       ls, d3d::device_error_word())
                 : d3d::launch_batch_step(
                       0, static_cast<d3d::BatchDesc*>(st.d_desc),
@@ -858,6 +886,19 @@ int d3d_server_set_kernel(d3d_server s, int kernel) {
       !s->res_pending.empty())
     return sfail(D3D_E_BUSY, "the step kernel changes only on an idle server");
   s->kernel = kernel;
+  return D3D_OK;
+}
+
+int d3d_server_set_large_kernel(d3d_server s, int kernel, int min_px) {
+  if (!s) return sfail(D3D_E_INVALID, "NULL server");
+  if (kernel > kMaxKernel || (kernel >= 0 && min_px < 1))
+    return sfail(D3D_E_INVALID, "no such large-solve kernel");
+  if (!s->queued.empty() || !s->active.empty() || !s->retiring.empty() ||
+      !s->res_pending.empty())
+    return sfail(D3D_E_BUSY,
+                 "the large-solve kernel changes only on an idle server");
+  s->large_kernel = kernel < 0 ? -1 : kernel;
+  s->large_px = min_px;
   return D3D_OK;
 }
 

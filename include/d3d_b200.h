@@ -369,6 +369,14 @@ int d3d_server_set_kernel(d3d_server server, int kernel);
  * for one another, so one stream's launch tail overlaps another's work. */
 int d3d_server_set_lanes(d3d_server server, int lanes);
 
+/* A second step kernel for large solves on an idle server (D3D_E_BUSY
+ * otherwise): solves whose pitched rows (ceil4(nx) floats) are at least
+ * min_px use `kernel` (0..6, the ids of d3d_server_set_kernel) on the
+ * upper half of the compute streams, the others the server's kernel on the
+ * lower half.  kernel < 0 turns it off (the default); it has no effect
+ * with the march kernel or a single stream. */
+int d3d_server_set_large_kernel(d3d_server server, int kernel, int min_px);
+
 /* Whether an idle server (D3D_E_BUSY otherwise) runs the solves that fit
  * the cluster-resident kernel on it (default off: on the 32..256 serving
  * stream it measured slower, the resident launches taking whole SMs from

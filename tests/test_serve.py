@@ -85,6 +85,35 @@ def test_every_step_kernel_bit_exact(kernel, lanes):
     assert B.check_device_errors() == 0
 
 
+@pytest.mark.parametrize("base,large,min_px,lanes", [(6, 2, 64, 4),
+                                                     (5, 1, 128, 2),
+                                                     (6, 2, 64, 1),
+                                                     (2, 6, 32, 3)])
+def test_large_solve_kernel_bit_exact(base, large, min_px, lanes):
+    """A second step kernel for the wide solves on their own lanes: every
+    result stays bit-exact, whichever side of the threshold a solve is."""
+    dims = [(1, 1, 1), (5, 33, 17), (61, 9, 35), (64, 16, 3), (130, 9, 35),
+            (131, 70, 6), (257, 5, 4), (36, 35, 70), (249, 11, 3),
+            (500, 7, 2), (127, 40, 20), (128, 3, 9)]
+    reqs = []
+    for i, (nx, ny, nz) in enumerate(dims):
+        c = B.batch_coefficients(nx, ny, nz, 0.05 + 0.01 * i)
+        f = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), 170 + i)
+        reqs.append((f, 1 + (i * 7) % 13, c))
+    server = B.Server(1 << 28, 4, base, lanes, False)
+    server.set_large_kernel(large, min_px)
+    outs = [np.full_like(f, np.nan) for f, _, _ in reqs]
+    for k, ((f, steps, c), o) in enumerate(zip(reqs, outs)):
+        server.submit(f, o, steps, c)
+        if k % 3 == 2:
+            server.tick()
+    server.drain()
+    server.close()
+    for (f, steps, c), o in zip(reqs, outs):
+        assert o.tobytes() == O.run(f, c, steps).tobytes()
+    assert B.check_device_errors() == 0
+
+
 def test_kernel_and_lanes_change_only_when_idle():
     server = B.Server(1 << 24, 4)
     f = np.zeros((4, 4, 5), np.float32)
