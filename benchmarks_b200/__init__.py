@@ -568,7 +568,7 @@ class Server:
         check(lib().d3d_server_set_kernel(self._h, int(kernel)))
 
     def set_lanes(self, lanes):
-        """Compute streams of the idle server (1..4, default 4)."""
+        """Compute streams of the idle server (1..8, default 4)."""
         check(lib().d3d_server_set_lanes(self._h, int(lanes)))
 
     def set_large_kernel(self, kernel, min_px=128):

@@ -47,7 +47,7 @@ constexpr int kMaxKernel = kStripBase + 1;
 int strip_nr(int kernel) {
   return kernel >= kStripBase ? kernel - kStripBase + 1 : 0;
 }
-constexpr int kMaxLanes = 4;               // compute streams
+constexpr int kMaxLanes = 8;               // compute streams
 // Step-kernel geometry of a kernel id: strip segments a thread (0 for the
 // tile forms and the march kernel) and, for the tile forms and the march
 // kernel, the xy tile.
@@ -905,7 +905,7 @@ int d3d_server_set_large_kernel(d3d_server s, int kernel, int min_px) {
 int d3d_server_set_lanes(d3d_server s, int lanes) {
   if (!s) return sfail(D3D_E_INVALID, "NULL server");
   if (lanes < 1 || lanes > kMaxLanes)
-    return sfail(D3D_E_INVALID, "lanes must be 1 to 4");
+    return sfail(D3D_E_INVALID, "lanes must be 1 to 8");
   if (!s->queued.empty() || !s->active.empty() || !s->retiring.empty() ||
       !s->res_pending.empty())
     return sfail(D3D_E_BUSY, "lanes change only on an idle server");

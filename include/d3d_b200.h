@@ -363,7 +363,7 @@ int d3d_server_tick(d3d_server server, long long* done_ids, int max_done,
  * of 4 floats, so it takes 2 * ceil4(nx)*ny*nz floats of the arena. */
 int d3d_server_set_kernel(d3d_server server, int kernel);
 
-/* Compute streams of an idle server (1..4, default 4; D3D_E_BUSY when
+/* Compute streams of an idle server (1..8, default 4; D3D_E_BUSY when
  * not idle).  Each solve runs all its steps on one stream, picked at
  * admission as the one with the least outstanding work; streams never wait
  * for one another, so one stream's launch tail overlaps another's work. */
