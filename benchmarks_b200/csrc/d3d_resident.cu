@@ -152,7 +152,8 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
   // Narrow thread shapes (2 units a thread) keep the rows above and below
   // as offsets and rotate three register sets through the b, c, t roles;
   // the wide ones (4 and 6 units) derive the row offsets from the flags and
-  // move c and t down a role each plane, which needs one register set less.
+  // keep only b in registers, loading c from shared memory each plane (one
+  // more load a segment, two register sets fewer).
   constexpr bool kWide = UMAX > 2;
   int c_off[UMAX], n_off[UMAX], s_off[UMAX];
   unsigned fl[UMAX];  // flag bits; bits 8..9: index of x = nx-1 if kCross
@@ -184,10 +185,12 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
       z0 > 0 ? map_to_rank(sm_base, rank - 1) + 4u * (pc - 1) * plane : 0u;
   const uint32_t above = z1 < nz ? map_to_rank(sm_base, rank + 1) : 0u;
 
-  // One plane of the march: b in vb, c in vc, t loaded into vt (three
-  // register sets whose roles rotate, so nothing is copied), the new values
-  // held until every thread of the CTA has read plane p, then stored over
-  // it.  Before the first store of a step, every CTA's pulls must be done.
+  // One plane of the march: b in vb, c in vc (narrow shapes; the wide ones
+  // load it), t loaded and kept in vt for the next plane (narrow: three
+  // register sets whose roles rotate, so nothing is copied; wide: vt is vb
+  // and receives c), the new values held until every thread of the CTA has
+  // read plane p, then stored over it.  Before the first store of a step,
+  // every CTA's pulls must be done.
   V16<float> q0[UMAX], q1[UMAX], q2[UMAX], nv[UMAX];
   auto plane_step = [&](int p, const V16<float>* vb, const V16<float>* vc,
                         V16<float>* vt) {
@@ -196,8 +199,8 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
 #pragma unroll
     for (int i = 0; i < UMAX; ++i) {
       const unsigned f = fl[i];
-      const V16<float> c = vc[i];
-      vt[i] = ld16_shared(tp + c_off[i]);
+      const V16<float> c = kWide ? ld16_shared(pl + c_off[i]) : vc[i];
+      const V16<float> t = ld16_shared(tp + c_off[i]);
       const int no = kWide ? c_off[i] - ((f & kNOwn) ? 0 : px) : n_off[i];
       const int sof = kWide ? c_off[i] + ((f & kSOwn) ? 0 : px) : s_off[i];
       const V16<float> n = ld16_shared(pl + no);
@@ -208,7 +211,7 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
       if (f & kWOwn) wl = c.e[0];
       er = ld_shared_if(f & kESm, pl + c_off[i] + 4, er);
       if (f & kEOwn) er = c.e[3];
-      V16<float> o = point_seg<float>(kk, c, n, so, vb[i], vt[i], wl, er);
+      V16<float> o = point_seg<float>(kk, c, n, so, vb[i], t, wl, er);
       if (f & kCross) {
         const unsigned jh = (f >> 8) & 3u;
         if (jh < 1) o.e[1] = o.e[0];
@@ -216,6 +219,9 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
         o.e[3] = o.e[2];
       }
       nv[i] = o;
+      // Narrow: t goes to the set that is c next plane.  Wide: c is the b
+      // of the next plane (vb and vt are the same set there).
+      vt[i] = kWide ? c : t;
     }
     __syncthreads();  // plane p read everywhere in this CTA
     if (p == 0) cluster_wait();  // every pull of the cluster is done
@@ -240,17 +246,13 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
     // before the wait, so the other CTAs' arrival overlaps that work.
     cluster_arrive();
     if (np > 0) {
+      if constexpr (!kWide) {
 #pragma unroll
-      for (int i = 0; i < UMAX; ++i) q1[i] = ld16_shared(sm + c_off[i]);
+        for (int i = 0; i < UMAX; ++i) q1[i] = ld16_shared(sm + c_off[i]);
+      }
       if constexpr (kWide) {
-        for (int p = 0; p < np; ++p) {
-          plane_step(p, q0, q1, q2);
-#pragma unroll
-          for (int i = 0; i < UMAX; ++i) {
-            q0[i] = q1[i];
-            q1[i] = q2[i];
-          }
-        }
+        // b in q0; each plane leaves its c there for the next.
+        for (int p = 0; p < np; ++p) plane_step(p, q0, q1, q0);
       } else {
         for (int p = 0; p < np; p += 3) {
           plane_step(p, q0, q1, q2);
