@@ -482,6 +482,8 @@ int plan_resident(d3d_batch b) {
     d.segs = segs;
     d.pc = pc;
     d.grid_id = i;
+    d.yparts = fit.yparts;
+    d.rows = fit.rows;
     for (int j = 0; j < 7; ++j) d.k[j] = g.coeff[j];
     d.k[7] = -0.0f;
     const std::pair<int, int> key(cl, v);

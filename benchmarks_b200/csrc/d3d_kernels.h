@@ -221,7 +221,8 @@ struct ResidentDesc {
   float* out;
   int nx, ny, nz, steps;
   int px, segs, pc, grid_id;
-  float k[8];  // ce, cw, cn, cs, ct, cb, cc, and -0.0
+  int yparts, rows;  // row parts of a plane (1, 2 or 4), rows in a part
+  float k[8];        // ce, cw, cn, cs, ct, cb, cc, and -0.0
 };
 // Thread shapes: `threads` a CTA, at most `units` 16-byte row segments of
 // a plane a thread (a plane of segs * ny segments fits when
@@ -234,14 +235,16 @@ constexpr int kResidentMaxCluster = 16;
 // Dynamic shared memory a CTA may hold: its pc planes and a halo plane.
 constexpr size_t kResidentSmemMax = 232448 - 1024;
 const ResidentVariant& resident_variant(int v);
-// Launch class of one grid on the resident kernel: the narrowest thread
-// shape that covers its ceil(nx/4) * ny row segments a plane and holds the
-// grid in at most 16 CTAs of pc planes plus a halo plane each, within the
-// shared memory a CTA of that shape may take -- a share of the SM for the
-// 128- and 256-thread shapes, so that 512 threads run on an SM.  False: no
+// Launch class of one grid on the resident kernel: a thread shape and a
+// cut of each plane into 1, 2 or 4 row parts (`rows` rows each) such that
+// a CTA's ceil(nx/4) * rows row segments are covered and the grid fits in
+// at most 16 CTAs (yparts row parts times z slabs of pc planes, plus a halo
+// plane each) within the shared memory a CTA of that shape may take -- a
+// share of the SM for the 128- and 256-thread shapes, so that 512 threads
+// run on an SM.  Narrow shapes and whole planes are preferred.  False: no
 // shape fits the grid.
 struct ResidentFit {
-  int cluster, variant, pc, px;
+  int cluster, variant, pc, px, yparts, rows;
   size_t smem;
 };
 bool resident_fit(int nx, int ny, int nz, ResidentFit* fit);

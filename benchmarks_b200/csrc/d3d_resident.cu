@@ -119,7 +119,9 @@ enum : unsigned {
   kESm = 16u,    // lane 31 inside a row: e is the staged word after
   kNOwn = 32u,   // y = 0: n is the own row
   kSOwn = 64u,   // y = ny-1: s is the own row
-  kCross = 128u  // the segment holds x = nx-1 followed by pads
+  kCross = 128u,  // the segment holds x = nx-1 followed by pads
+  kPullN = 1024u,  // first row of a part not at y = 0: pulls the y halo below
+  kPullS = 2048u   // last row of a part not at y = ny-1: pulls the one above
 };
 
 template <int NT, int UMAX>
@@ -130,25 +132,37 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
   const int tid = threadIdx.x, lane = tid & 31;
   const int nx = d.nx, ny = d.ny, nz = d.nz, px = d.px, S = d.segs;
   const int pc = d.pc;
-  const int plane = px * ny;
-  const int z0 = (int)rank * pc;
+  // Cluster rank = zk * yparts + yk: rows [y0, y0 + yn) of planes
+  // [z0, z1).  With row parts (yparts > 1) a plane in shared memory is
+  // rows + 2 rows of px floats: row 0 and row rows + 1 hold the
+  // neighbouring parts' edge rows (the y halo), rows 1..yn this CTA's rows;
+  // whole planes (yparts = 1) have no halo rows.  Every CTA of the grid has
+  // the same layout (rows = ceil(ny / yparts)), so a neighbour's plane p
+  // starts at the same offset.
+  const int yparts = d.yparts, rows = d.rows;
+  const int yk = (int)rank % yparts, zk = (int)rank / yparts;
+  const int y0 = yk * rows;
+  const int yn = max(0, min(ny, y0 + rows) - y0);
+  const int hrow = yparts > 1 ? 1 : 0;  // first row of the CTA's own rows
+  const int plane = px * (rows + 2 * hrow);
+  const int z0 = zk * pc;
   const int z1 = min(nz, z0 + pc);
-  const int np = max(0, z1 - z0);
+  const int np = yn > 0 ? max(0, z1 - z0) : 0;
   float* halo = sm + pc * plane;  // the plane above the slab (t of z1-1)
 
   // Load the slab: rows of nx floats into rows of px, pads from nx-1.
   {
-    const float* __restrict__ src = d.in + (size_t)z0 * ny * nx;
-    const int rows = np * ny;
-    for (int r = tid >> 5; r < rows; r += NT / 32) {
-      const float* in = src + (size_t)r * nx;
-      float* o = sm + r * px;
+    const int nrow = np * yn;
+    for (int r = tid >> 5; r < nrow; r += NT / 32) {
+      const int zz = r / yn, yy = r - zz * yn;
+      const float* in = d.in + ((size_t)(z0 + zz) * ny + y0 + yy) * nx;
+      float* o = sm + zz * plane + (yy + hrow) * px;
       for (int x = lane; x < px; x += 32) o[x] = in[min(x, nx - 1)];
     }
   }
 
   // This thread's units u = tid + i * NT of the plane (S segments a row).
-  const int units = S * ny;
+  const int units = S * yn;
   // Narrow thread shapes (2 units a thread) keep the rows above and below
   // as offsets and rotate three register sets through the b, c, t roles;
   // the wide ones (4 and 6 units) derive the row offsets from the flags and
@@ -162,18 +176,22 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
     const int u = tid + i * NT;
     const bool valid = u < units;
     const int uu = valid ? u : 0;
-    const int y = uu / S, seg = uu - y * S;
-    const int xg = 4 * seg;
-    c_off[i] = y * px + xg;
-    n_off[i] = y == 0 ? c_off[i] : c_off[i] - px;        // y = 0: own row
-    s_off[i] = y == ny - 1 ? c_off[i] : c_off[i] + px;   // y = ny-1: own row
+    const int r = uu / S, seg = uu - r * S;  // r: row within the part
+    const int yg = y0 + r, xg = 4 * seg;
+    c_off[i] = (r + hrow) * px + xg;
+    // y = 0 / ny-1 read their own row; a part's edge row reads the halo
+    // row the pull fills.
+    n_off[i] = yg == 0 ? c_off[i] : c_off[i] - px;
+    s_off[i] = yg == ny - 1 ? c_off[i] : c_off[i] + px;
     unsigned f = valid ? kValid : 0u;
     if (seg == 0) f |= kWOwn;
     else if (lane == 0) f |= kWSm;
     if (seg == S - 1) f |= kEOwn;
     else if (lane == 31) f |= kESm;
-    if (y == 0) f |= kNOwn;
-    if (y == ny - 1) f |= kSOwn;
+    if (yg == 0) f |= kNOwn;
+    if (yg == ny - 1) f |= kSOwn;
+    if (valid && r == 0 && yg > 0) f |= kPullN;
+    if (valid && r == yn - 1 && yg < ny - 1) f |= kPullS;
     if (xg + 4 > nx) f |= kCross | ((unsigned)(nx - 1 - xg) << 8);
     fl[i] = f;
   }
@@ -181,9 +199,20 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
                       d.k[4], d.k[5], d.k[6], d.k[7]};
   const Coef2 kk = coef2(k);
   const uint32_t sm_base = smem_u32(sm);
+  // z neighbours: the same rows of the slabs below and above (ranks
+  // -/+ yparts); y neighbours: the parts before and after (ranks -/+ 1).
   const uint32_t below =
-      z0 > 0 ? map_to_rank(sm_base, rank - 1) + 4u * (pc - 1) * plane : 0u;
-  const uint32_t above = z1 < nz ? map_to_rank(sm_base, rank + 1) : 0u;
+      z0 > 0 ? map_to_rank(sm_base, rank - yparts) + 4u * (pc - 1) * plane
+             : 0u;
+  const uint32_t above = z1 < nz ? map_to_rank(sm_base, rank + yparts) : 0u;
+  // The part before is full and ends with row `rows` of its layout; the
+  // part after starts with row 1.  Their rows land in this CTA's rows 0
+  // and yn + 1: for a first-row unit (row 1, c_off = px + x) the source is
+  // the part before's row `rows` at x, for a last-row unit (row yn,
+  // c_off = yn * px + x) the part after's row 1 at x.
+  const uint32_t ybelow = yk > 0 ? map_to_rank(sm_base, rank - 1) : 0u;
+  const uint32_t yabove =
+      yk + 1 < yparts && y0 + yn < ny ? map_to_rank(sm_base, rank + 1) : 0u;
 
   // One plane of the march: b in vb, c in vc (narrow shapes; the wide ones
   // load it), t loaded and kept in vt for the next plane (narrow: three
@@ -240,6 +269,18 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
                        : ld16_shared(sm + c_off[i]);
         if (z1 < nz && (fl[i] & kValid))
           st16_shared(halo + c_off[i], ld16_cluster(above + 4u * c_off[i]));
+        // y halo of every plane of the slab: the row under a part's first
+        // row, the row over its last row (old values, as the z halo).
+        if (fl[i] & kPullN)
+          for (int p = 0; p < np; ++p)
+            st16_shared(sm + p * plane + c_off[i] - px,
+                        ld16_cluster(ybelow + 4u * (p * plane + rows * px +
+                                                    c_off[i] - px)));
+        if (fl[i] & kPullS)
+          for (int p = 0; p < np; ++p)
+            st16_shared(sm + p * plane + c_off[i] + px,
+                        ld16_cluster(yabove + 4u * (p * plane + px +
+                                                    c_off[i] - yn * px)));
       }
     }
     // This thread's pulls are done; the new values of plane 0 are computed
@@ -273,18 +314,16 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
   __syncthreads();
   // Store the slab: the first nx floats of each row.
   {
-    float* __restrict__ dst = d.out + (size_t)z0 * ny * nx;
-    const int rows = np * ny;
-    for (int r = tid >> 5; r < rows; r += NT / 32) {
-      float* o = dst + (size_t)r * nx;
-      const float* in = sm + r * px;
+    const int nrow = np * yn;
+    for (int r = tid >> 5; r < nrow; r += NT / 32) {
+      const int zz = r / yn, yy = r - zz * yn;
+      float* o = d.out + ((size_t)(z0 + zz) * ny + y0 + yy) * nx;
+      const float* in = sm + zz * plane + (yy + hrow) * px;
       for (int x = lane; x < nx; x += 32) o[x] = in[x];
     }
   }
 }
 
-// The narrow shapes run several CTAs an SM (512 threads in all): their
-// registers are capped to fit.
 template <int NT, int UMAX>
 __global__ void __launch_bounds__(NT, (NT < 512 ? 512 / NT : 1))
     resident_kernel(const ResidentDesc* __restrict__ descs, int ngrids,
@@ -373,29 +412,41 @@ const ResidentVariant& resident_variant(int v) { return kResident[v]; }
 
 bool resident_fit(int nx, int ny, int nz, ResidentFit* fit) {
   const int px = (nx + 3) / 4 * 4, segs = px / 4;
-  const long long plane = (long long)px * ny;
-  const long long units = (long long)segs * ny;
-  // Thread shapes in order of preference, narrowest first: a narrow shape
-  // takes a share of the SM's shared memory so that 512 threads (several
-  // CTAs of different clusters) run on an SM and one CTA's barrier waits
-  // overlap another's work.  The first shape that covers the plane and
-  // needs at most 16 CTAs at its share wins; the 512- and 384-thread shapes
-  // take a whole SM.  (A 256-thread shape with 4 units a thread at half an
-  // SM measured 10-17% slower on B200 than 512 threads with 2 units at a
-  // whole SM, at 48^3 and 64^3.)
-  for (int v = 0; v < kNumResidentVariants; ++v) {
-    const ResidentVariant& rv = kResident[v];
+  // Candidates in order of preference: the narrow thread shapes (2 units a
+  // thread; 128 and 256 threads take a share of the SM's shared memory so
+  // that 512 threads run on an SM and one CTA's barrier waits overlap
+  // another's work) with whole planes, then with planes cut into 2 or 4
+  // row parts (each CTA holds its rows plus one halo row on each side); the
+  // wide shapes (4 and 6 units a thread, whole planes) last.  The first
+  // that covers a CTA's plane and needs at most 16 CTAs wins.  (On B200 the
+  // wide shapes ran 80^3 at 450 Gpt/s against 710 for 64^3 on the 512-thread
+  // narrow shape; a 256-thread shape with 4 units at half an SM measured
+  // slower than 512 threads with 2 at a whole SM.)
+  struct Cand {
+    int v, yparts;
+  };
+  static const Cand cands[] = {{0, 1}, {1, 1}, {2, 1}, {0, 2}, {1, 2},
+                               {2, 2}, {0, 4}, {1, 4}, {2, 4}, {3, 1},
+                               {4, 1}};
+  for (const Cand& cd : cands) {
+    const ResidentVariant& rv = kResident[cd.v];
+    if (cd.yparts > 1 && ny < 8 * cd.yparts) continue;
+    const int rows = (ny + cd.yparts - 1) / cd.yparts;
+    const long long units = (long long)segs * rows;
     if (units > (long long)rv.threads * rv.units) continue;
+    const long long plane = (long long)px * (rows + (cd.yparts > 1 ? 2 : 0));
     const int per_sm = std::max(1, 512 / rv.threads);
     const size_t cap =
         std::min(kResidentSmemMax, (size_t)(233472 / per_sm) - 1024);
     const long long pmax = (long long)(cap / 4) / plane - 1;
     if (pmax < 1) continue;
-    const int cl = (int)((nz + pmax - 1) / pmax);
-    if (cl > kResidentMaxCluster) continue;
-    fit->cluster = cl;
-    fit->variant = v;
-    fit->pc = (nz + cl - 1) / cl;
+    const int zparts = (int)((nz + pmax - 1) / pmax);
+    if (zparts * cd.yparts > kResidentMaxCluster) continue;
+    fit->cluster = zparts * cd.yparts;
+    fit->variant = cd.v;
+    fit->yparts = cd.yparts;
+    fit->rows = rows;
+    fit->pc = (nz + zparts - 1) / zparts;
     fit->smem = (size_t)((fit->pc + 1) * plane * 4);
     fit->px = px;
     return true;

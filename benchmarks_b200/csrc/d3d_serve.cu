@@ -109,7 +109,7 @@ struct Request {
   // Cluster-resident solve: one dense buffer (off_a), its launch class
   // (cluster size, thread shape) and shared memory, planes per CTA.
   bool resident = false;
-  int r_cluster = 0, r_variant = 0, r_pc = 0;
+  int r_cluster = 0, r_variant = 0, r_pc = 0, r_yparts = 1, r_rows = 0;
   size_t r_smem = 0;
   int nx, ny, nz, steps, done;
   int px;  // row pitch in floats (nx, or nx rounded up to 4 when pitched)
@@ -275,6 +275,8 @@ void plan_resident_solve(d3d_server s, Request* r) {
   r->r_cluster = cl;
   r->r_variant = v;
   r->r_pc = pc;
+  r->r_yparts = fit.yparts;
+  r->r_rows = fit.rows;
   r->r_smem = smem;
   r->px = r->nx;  // one dense buffer
 }
@@ -485,6 +487,8 @@ int launch_resident_group(d3d_server s) {
     d.segs = d.px / 4;
     d.pc = r->r_pc;
     d.grid_id = (int)i;
+    d.yparts = r->r_yparts;
+    d.rows = r->r_rows;
     for (int j = 0; j < 7; ++j) d.k[j] = r->coeff[j];
     d.k[7] = -0.0f;
     S_TRY(cudaStreamWaitEvent(s->res_stream, r->ev_in, 0),

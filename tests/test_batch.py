@@ -242,16 +242,18 @@ def test_more_grids_than_one_launch_row():
 
 
 # Grids for the cluster-resident kernel.  A CTA holds at most 57,856 floats:
-# pc planes of ceil4(nx) * ny and one halo plane, so a grid needs
-# ceil(nz / (57856 // plane - 1)) CTAs.  These cover clusters of 1 to 16
-# CTAs, a last CTA with fewer planes, one-plane slabs, every thread shape
-# (plane segments up to 256, 512, 1024, 2048 and 2304), rows of one
-# segment, nx leaving 0..3 pad columns, and grids it does not fit (too
-# many CTAs; too many segments a plane), which run on the strip kind.
+# pc planes (or their row parts, with a halo row on each side) and one halo
+# plane, in at most 16 CTAs.  These cover clusters of 1 to 16 CTAs, a last
+# CTA with fewer planes, one-plane slabs, planes cut into 2 and 4 row parts
+# (a last part with fewer rows), every thread shape (the 512 x 4 and
+# 384 x 6 ones for wide planes of few rows), rows of one segment, nx
+# leaving 0..3 pad columns, and a grid it does not fit (96^3: 20 CTAs),
+# which runs on the strip kind.
 RESIDENT_DIMS = [(1, 1, 1), (5, 1, 9), (17, 23, 5), (13, 1, 30),
                  (64, 64, 64), (88, 80, 37), (96, 96, 80), (95, 7, 300),
                  (33, 60, 45), (96, 90, 12), (40, 40, 200), (96, 96, 96),
-                 (100, 96, 10), (57, 31, 128), (16, 96, 96), (96, 16, 3)]
+                 (100, 96, 10), (57, 31, 128), (16, 96, 96), (96, 16, 3),
+                 (500, 9, 20), (700, 12, 11), (93, 67, 40)]
 
 
 def _resident_specs(steps_of):
@@ -272,9 +274,9 @@ def test_cluster_resident_kind_bit_exact_with_step_counters():
     info = batch.info()
     res = info["resident"]
     assert res["on"]
-    # (96, 96, 96) needs 20 CTAs and (100, 96, 10) 2400 segments a plane:
-    # those two run on the strip kind, every other grid on the resident one
-    assert res["grids"] == len(specs) - 2
+    # (96, 96, 96) needs 20 CTAs: it runs on the strip kind, every other
+    # grid on the resident one
+    assert res["grids"] == len(specs) - 1
     clusters = {c["cluster"] for c in res["classes"]}
     assert 1 in clusters and 16 in clusters
     assert {c["threads"] for c in res["classes"]} == {128, 256, 512, 384}
