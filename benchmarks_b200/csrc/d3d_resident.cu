@@ -123,6 +123,7 @@ enum : unsigned {
   kPullN = 1024u,  // first row of a part not at y = 0: pulls the y halo below
   kPullS = 2048u   // last row of a part not at y = ny-1: pulls the one above
 };
+constexpr int kYBatch = 4;  // y-halo planes pulled per batch of loads
 
 template <int NT, int UMAX>
 __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
@@ -263,24 +264,41 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
   for (int s = 0; s < d.steps; ++s) {
     cluster_wait();  // planes of the previous step complete everywhere
     if (np > 0) {
+      // Every remote load of a batch is issued before any of its values is
+      // stored, so the loads' latencies overlap instead of adding up.
+      V16<float> tv[UMAX];
 #pragma unroll
       for (int i = 0; i < UMAX; ++i) {
         q0[i] = z0 > 0 ? ld16_cluster(below + 4u * c_off[i])
                        : ld16_shared(sm + c_off[i]);
-        if (z1 < nz && (fl[i] & kValid))
-          st16_shared(halo + c_off[i], ld16_cluster(above + 4u * c_off[i]));
-        // y halo of every plane of the slab: the row under a part's first
-        // row, the row over its last row (old values, as the z halo).
-        if (fl[i] & kPullN)
-          for (int p = 0; p < np; ++p)
-            st16_shared(sm + p * plane + c_off[i] - px,
-                        ld16_cluster(ybelow + 4u * (p * plane + rows * px +
-                                                    c_off[i] - px)));
-        if (fl[i] & kPullS)
-          for (int p = 0; p < np; ++p)
-            st16_shared(sm + p * plane + c_off[i] + px,
-                        ld16_cluster(yabove + 4u * (p * plane + px +
-                                                    c_off[i] - yn * px)));
+        if (z1 < nz) tv[i] = ld16_cluster(above + 4u * c_off[i]);
+      }
+      if (z1 < nz) {
+#pragma unroll
+        for (int i = 0; i < UMAX; ++i)
+          if (fl[i] & kValid) st16_shared(halo + c_off[i], tv[i]);
+      }
+      // y halo of every plane of the slab: the row under a part's first
+      // row, the row over its last row (old values, as the z halo), in
+      // batches of kYBatch planes.
+#pragma unroll
+      for (int i = 0; i < UMAX; ++i) {
+        if (!(fl[i] & (kPullN | kPullS))) continue;
+        const bool dn = fl[i] & kPullN;
+        const int dst = dn ? c_off[i] - px : c_off[i] + px;
+        const uint32_t src =
+            dn ? ybelow + 4u * (rows * px + c_off[i] - px)
+               : yabove + 4u * (px + c_off[i] - yn * px);
+        for (int p0 = 0; p0 < np; p0 += kYBatch) {
+          V16<float> yv[kYBatch];
+#pragma unroll
+          for (int j = 0; j < kYBatch; ++j)
+            if (p0 + j < np)
+              yv[j] = ld16_cluster(src + 4u * (p0 + j) * plane);
+#pragma unroll
+          for (int j = 0; j < kYBatch; ++j)
+            if (p0 + j < np) st16_shared(sm + (p0 + j) * plane + dst, yv[j]);
+        }
       }
     }
     // This thread's pulls are done; the new values of plane 0 are computed
