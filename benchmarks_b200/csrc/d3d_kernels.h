@@ -231,6 +231,9 @@ struct ResidentVariant {
   int threads, units;
 };
 constexpr int kNumResidentVariants = 5;
+// Launch variant ids: the shape index, plus kResidentParts for the build
+// with row parts (shapes 0..2 only).
+constexpr int kResidentParts = kNumResidentVariants;
 constexpr int kResidentMaxCluster = 16;
 // Dynamic shared memory a CTA may hold: its pc planes and a halo plane.
 constexpr size_t kResidentSmemMax = 232448 - 1024;

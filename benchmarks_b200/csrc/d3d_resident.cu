@@ -125,7 +125,9 @@ enum : unsigned {
 };
 constexpr int kYBatch = 4;  // y-halo planes pulled per batch of loads
 
-template <int NT, int UMAX>
+// PARTS: the grid's planes are cut into row parts (d.yparts > 1); without
+// it the code for the y halo is left out.
+template <int NT, int UMAX, bool PARTS>
 __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
                                               unsigned rank, float* sm,
                                               int* __restrict__ steps_done,
@@ -140,11 +142,11 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
   // whole planes (yparts = 1) have no halo rows.  Every CTA of the grid has
   // the same layout (rows = ceil(ny / yparts)), so a neighbour's plane p
   // starts at the same offset.
-  const int yparts = d.yparts, rows = d.rows;
+  const int yparts = PARTS ? d.yparts : 1, rows = PARTS ? d.rows : ny;
   const int yk = (int)rank % yparts, zk = (int)rank / yparts;
   const int y0 = yk * rows;
   const int yn = max(0, min(ny, y0 + rows) - y0);
-  const int hrow = yparts > 1 ? 1 : 0;  // first row of the CTA's own rows
+  const int hrow = PARTS ? 1 : 0;  // first row of the CTA's own rows
   const int plane = px * (rows + 2 * hrow);
   const int z0 = zk * pc;
   const int z1 = min(nz, z0 + pc);
@@ -264,25 +266,19 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
   for (int s = 0; s < d.steps; ++s) {
     cluster_wait();  // planes of the previous step complete everywhere
     if (np > 0) {
-      // Every remote load of a batch is issued before any of its values is
-      // stored, so the loads' latencies overlap instead of adding up.
-      V16<float> tv[UMAX];
 #pragma unroll
       for (int i = 0; i < UMAX; ++i) {
         q0[i] = z0 > 0 ? ld16_cluster(below + 4u * c_off[i])
                        : ld16_shared(sm + c_off[i]);
-        if (z1 < nz) tv[i] = ld16_cluster(above + 4u * c_off[i]);
-      }
-      if (z1 < nz) {
-#pragma unroll
-        for (int i = 0; i < UMAX; ++i)
-          if (fl[i] & kValid) st16_shared(halo + c_off[i], tv[i]);
+        if (z1 < nz && (fl[i] & kValid))
+          st16_shared(halo + c_off[i], ld16_cluster(above + 4u * c_off[i]));
       }
       // y halo of every plane of the slab: the row under a part's first
       // row, the row over its last row (old values, as the z halo), in
-      // batches of kYBatch planes.
+      // batches of kYBatch planes whose remote loads are all issued before
+      // any is stored, so their latencies overlap.
 #pragma unroll
-      for (int i = 0; i < UMAX; ++i) {
+      for (int i = 0; i < UMAX && PARTS; ++i) {
         if (!(fl[i] & (kPullN | kPullS))) continue;
         const bool dn = fl[i] & kPullN;
         const int dst = dn ? c_off[i] - px : c_off[i] + px;
@@ -342,7 +338,7 @@ __device__ __forceinline__ void resident_grid(const ResidentDesc& d,
   }
 }
 
-template <int NT, int UMAX>
+template <int NT, int UMAX, bool PARTS>
 __global__ void __launch_bounds__(NT, (NT < 512 ? 512 / NT : 1))
     resident_kernel(const ResidentDesc* __restrict__ descs, int ngrids,
                     unsigned* __restrict__ queue,
@@ -359,7 +355,7 @@ __global__ void __launch_bounds__(NT, (NT < 512 ? 512 / NT : 1))
                                   smem_u32(&next_grid), 0));
     cluster_sync_all();  // everyone has read it before rank 0 rewrites it
     if (g >= ngrids) break;
-    resident_grid<NT, UMAX>(descs[g], rank, sm, steps_done,
+    resident_grid<NT, UMAX, PARTS>(descs[g], rank, sm, steps_done,
                             descs[g].grid_id);
   }
 }
@@ -369,11 +365,11 @@ __global__ void __launch_bounds__(NT, (NT < 512 ? 512 / NT : 1))
 const ResidentVariant kResident[kNumResidentVariants] = {
     {128, 2}, {256, 2}, {512, 2}, {512, 4}, {384, 6}};
 
-template <int NT, int UMAX>
+template <int NT, int UMAX, bool PARTS>
 cudaError_t launch_v(const ResidentDesc* descs, int ngrids, unsigned* queue,
                      int* steps_done, int cluster, int nclusters,
                      size_t smem, cudaStream_t s) {
-  auto kern = resident_kernel<NT, UMAX>;
+  auto kern = resident_kernel<NT, UMAX, PARTS>;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(nclusters * cluster));
   cfg.blockDim = dim3(NT);
@@ -389,9 +385,9 @@ cudaError_t launch_v(const ResidentDesc* descs, int ngrids, unsigned* queue,
   return cudaLaunchKernelEx(&cfg, kern, descs, ngrids, queue, steps_done);
 }
 
-template <int NT, int UMAX>
+template <int NT, int UMAX, bool PARTS>
 cudaError_t prepare_v() {
-  auto kern = resident_kernel<NT, UMAX>;
+  auto kern = resident_kernel<NT, UMAX, PARTS>;
   cudaError_t e = cudaFuncSetAttribute(
       kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
       (int)kResidentSmemMax);
@@ -400,9 +396,9 @@ cudaError_t prepare_v() {
       kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
 }
 
-template <int NT, int UMAX>
+template <int NT, int UMAX, bool PARTS>
 cudaError_t max_clusters_v(int cluster, size_t smem, int* out) {
-  auto kern = resident_kernel<NT, UMAX>;
+  auto kern = resident_kernel<NT, UMAX, PARTS>;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)cluster);
   cfg.blockDim = dim3(NT);
@@ -426,7 +422,9 @@ __global__ void set_counters_kernel(const int2* __restrict__ id_steps, int n,
 
 }  // namespace
 
-const ResidentVariant& resident_variant(int v) { return kResident[v]; }
+const ResidentVariant& resident_variant(int v) {
+  return kResident[v % kResidentParts];
+}
 
 bool resident_fit(int nx, int ny, int nz, ResidentFit* fit) {
   const int px = (nx + 3) / 4 * 4, segs = px / 4;
@@ -461,7 +459,7 @@ bool resident_fit(int nx, int ny, int nz, ResidentFit* fit) {
     const int zparts = (int)((nz + pmax - 1) / pmax);
     if (zparts * cd.yparts > kResidentMaxCluster) continue;
     fit->cluster = zparts * cd.yparts;
-    fit->variant = cd.v;
+    fit->variant = cd.v + (cd.yparts > 1 ? kResidentParts : 0);
     fit->yparts = cd.yparts;
     fit->rows = rows;
     fit->pc = (nz + zparts - 1) / zparts;
@@ -486,11 +484,14 @@ cudaError_t resident_prepare() {
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (done_dev == dev) return cudaSuccess;
-  if ((e = prepare_v<128, 2>()) != cudaSuccess) return e;
-  if ((e = prepare_v<256, 2>()) != cudaSuccess) return e;
-  if ((e = prepare_v<512, 2>()) != cudaSuccess) return e;
-  if ((e = prepare_v<512, 4>()) != cudaSuccess) return e;
-  if ((e = prepare_v<384, 6>()) != cudaSuccess) return e;
+  if ((e = prepare_v<128, 2, false>()) != cudaSuccess) return e;
+  if ((e = prepare_v<256, 2, false>()) != cudaSuccess) return e;
+  if ((e = prepare_v<512, 2, false>()) != cudaSuccess) return e;
+  if ((e = prepare_v<512, 4, false>()) != cudaSuccess) return e;
+  if ((e = prepare_v<384, 6, false>()) != cudaSuccess) return e;
+  if ((e = prepare_v<128, 2, true>()) != cudaSuccess) return e;
+  if ((e = prepare_v<256, 2, true>()) != cudaSuccess) return e;
+  if ((e = prepare_v<512, 2, true>()) != cudaSuccess) return e;
   done_dev = dev;
   return cudaSuccess;
 }
@@ -499,11 +500,14 @@ cudaError_t resident_max_clusters(int variant, int cluster, size_t smem,
                                   int* out) {
   *out = 0;
   switch (variant) {
-    case 0: return max_clusters_v<128, 2>(cluster, smem, out);
-    case 1: return max_clusters_v<256, 2>(cluster, smem, out);
-    case 2: return max_clusters_v<512, 2>(cluster, smem, out);
-    case 3: return max_clusters_v<512, 4>(cluster, smem, out);
-    case 4: return max_clusters_v<384, 6>(cluster, smem, out);
+    case 0: return max_clusters_v<128, 2, false>(cluster, smem, out);
+    case 1: return max_clusters_v<256, 2, false>(cluster, smem, out);
+    case 2: return max_clusters_v<512, 2, false>(cluster, smem, out);
+    case 3: return max_clusters_v<512, 4, false>(cluster, smem, out);
+    case 4: return max_clusters_v<384, 6, false>(cluster, smem, out);
+    case kResidentParts + 0: return max_clusters_v<128, 2, true>(cluster, smem, out);
+    case kResidentParts + 1: return max_clusters_v<256, 2, true>(cluster, smem, out);
+    case kResidentParts + 2: return max_clusters_v<512, 2, true>(cluster, smem, out);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -517,11 +521,14 @@ cudaError_t launch_resident(int variant, const ResidentDesc* descs,
       smem > kResidentSmemMax)
     return cudaErrorInvalidValue;
   switch (variant) {
-    case 0: return launch_v<128, 2>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
-    case 1: return launch_v<256, 2>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
-    case 2: return launch_v<512, 2>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
-    case 3: return launch_v<512, 4>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
-    case 4: return launch_v<384, 6>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case 0: return launch_v<128, 2, false>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case 1: return launch_v<256, 2, false>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case 2: return launch_v<512, 2, false>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case 3: return launch_v<512, 4, false>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case 4: return launch_v<384, 6, false>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case kResidentParts + 0: return launch_v<128, 2, true>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case kResidentParts + 1: return launch_v<256, 2, true>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
+    case kResidentParts + 2: return launch_v<512, 2, true>(descs, ngrids, queue, steps_done, cluster, nclusters, smem, s);
     default: return cudaErrorInvalidValue;
   }
 }

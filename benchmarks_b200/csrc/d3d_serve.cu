@@ -142,7 +142,7 @@ struct ResStaging {
   bool in_flight = false;
 };
 constexpr int kMaxResClasses =
-    d3d::kResidentMaxCluster * d3d::kNumResidentVariants;
+    d3d::kResidentMaxCluster * (d3d::kResidentParts + 3);
 
 // Staging for one tick's descriptors (BatchDesc or PitchedDesc, by the
 // server's kernel) and work items, pinned + device.
