@@ -139,10 +139,14 @@ struct ResStaging {
   size_t cap = 0;
   unsigned* d_queue = nullptr;  // kMaxResClasses counters
   cudaEvent_t done = nullptr;
+  cudaStream_t stream = nullptr;  // descriptors in, launches joined
   bool in_flight = false;
 };
 constexpr int kMaxResClasses =
     d3d::kResidentMaxCluster * (d3d::kResidentParts + 3);
+constexpr int kResStages = 16;         // group stagings in the ring
+constexpr size_t kResGroupCap = 256;   // solves per group launch
+constexpr int kResStreams = 16;        // streams the launches run on
 
 // Staging for one tick's descriptors (BatchDesc or PitchedDesc, by the
 // server's kernel) and work items, pinned + device.
@@ -190,10 +194,16 @@ struct d3d_server_s {
   // launch; the stream and stagings of those launches.
   bool resident = false;
   std::vector<Request*> res_pending;
-  cudaStream_t res_stream = nullptr;
-  // Group stagings: one is reused only once its launches have ended (an
-  // event query, never a host wait), so a long small solve does not hold
-  // up the ticks; a new one is made when none is free.
+  cudaStream_t res_pool[kResStreams] = {};
+  cudaEvent_t res_join[kResStreams] = {};
+  cudaEvent_t res_ready = nullptr;
+  int res_rr = 0;
+  // Group stagings: a fixed ring made when the resident path is switched
+  // on.  Allocating while serving would serialise the lanes (a page-locked
+  // or device allocation keeps work issued to different streams before and
+  // after it from overlapping).  A staging is reused only once its launches
+  // have ended (an event query, never a host wait), so a long small solve
+  // does not hold up the ticks; with none free, the group waits a tick.
   std::vector<ResStaging*> rstage;
   long long res_solves = 0, res_launches = 0;
   std::map<std::tuple<int, int, size_t>, int> res_max_clusters;
@@ -423,8 +433,12 @@ int admit(d3d_server s) {
 
 // Launches every cluster-resident solve admitted since the last group:
 // one persistent launch per (cluster size, thread shape), largest work
-// first, on the resident stream after the solves' input copies; each
-// result is copied out once the group's launches end.
+// first.  A launch lasts as long as its longest solve (its steps run one
+// after another), so each goes on an idle stream of the resident pool,
+// after its solves' input copies, and groups overlap; each result is
+// copied out on the same stream once its launch ends.  The group's
+// descriptors travel on its staging's own stream, which joins the
+// launches' streams to mark the staging free again.
 int launch_resident_group(d3d_server s) {
   if (s->res_pending.empty()) return D3D_OK;
   ResStaging* free_st = nullptr;
@@ -438,11 +452,7 @@ int launch_resident_group(d3d_server s) {
     free_st = c;
     break;
   }
-  if (!free_st) {
-    free_st = new (std::nothrow) ResStaging();
-    if (!free_st) return sfail(D3D_E_OOM, "resident staging");
-    s->rstage.push_back(free_st);
-  }
+  if (!free_st) return D3D_OK;  // every staging busy: a later tick launches
   ResStaging& st = *free_st;
   std::vector<Request*>& list = s->res_pending;
   std::stable_sort(list.begin(), list.end(), [](const Request* x,
@@ -452,28 +462,9 @@ int launch_resident_group(d3d_server s) {
     return (double)x->nx * x->ny * x->nz * x->steps >
            (double)y->nx * y->ny * y->nz * y->steps;
   });
-  const size_t n = list.size();
-  if (n > st.cap) {
-    if (st.h) cudaFreeHost(st.h);
-    if (st.d) cudaFree(st.d);
-    if (st.d_steps) cudaFree(st.d_steps);
-    st.h = nullptr;
-    st.d = nullptr;
-    st.d_steps = nullptr;
-    st.cap = std::max({n, 2 * st.cap, (size_t)256});
-    S_TRY(cudaMallocHost(&st.h, st.cap * sizeof(d3d::ResidentDesc)),
-          "cudaMallocHost (resident staging)");
-    S_TRY(cudaMalloc(&st.d, st.cap * sizeof(d3d::ResidentDesc)),
-          "cudaMalloc (resident staging)");
-    S_TRY(cudaMalloc(&st.d_steps, st.cap * sizeof(int)),
-          "cudaMalloc (resident step counters)");
-  }
-  if (!st.d_queue) {
-    S_TRY(cudaMalloc(&st.d_queue, kMaxResClasses * sizeof(unsigned)),
-          "cudaMalloc (resident work counters)");
-    S_TRY(cudaEventCreateWithFlags(&st.done, cudaEventDisableTiming),
-          "cudaEventCreate");
-  }
+  // At most one staging's worth; the rest wait for the next group.  The
+  // first `n` of the sorted list are still grouped by class.
+  const size_t n = std::min(list.size(), st.cap);
   for (size_t i = 0; i < n; ++i) {
     const Request* r = list[i];
     d3d::ResidentDesc& d = st.h[i];
@@ -491,16 +482,15 @@ int launch_resident_group(d3d_server s) {
     d.rows = r->r_rows;
     for (int j = 0; j < 7; ++j) d.k[j] = r->coeff[j];
     d.k[7] = -0.0f;
-    S_TRY(cudaStreamWaitEvent(s->res_stream, r->ev_in, 0),
-          "cudaStreamWaitEvent");
   }
-  cudaStream_t rs = s->res_stream;
+  const cudaStream_t gs = st.stream;
   S_TRY(cudaMemcpyAsync(st.d, st.h, n * sizeof(d3d::ResidentDesc),
-                        cudaMemcpyHostToDevice, rs),
+                        cudaMemcpyHostToDevice, gs),
         "H2D resident descriptors");
   S_TRY(cudaMemsetAsync(st.d_queue, 0, kMaxResClasses * sizeof(unsigned),
-                        rs),
+                        gs),
         "work counter reset");
+  S_TRY(cudaEventRecord(s->res_ready, gs), "cudaEventRecord");
   int ci = 0;
   for (size_t b = 0; b < n; ++ci) {
     size_t e = b;
@@ -510,33 +500,49 @@ int launch_resident_group(d3d_server s) {
       smem = std::max(smem, list[e]->r_smem);
       ++e;
     }
+    // The first idle stream of the pool, else the next one in turn.
+    int p = -1;
+    for (int k = 0; k < kResStreams && p < 0; ++k) {
+      const int c = (s->res_rr + k) % kResStreams;
+      if (cudaStreamQuery(s->res_pool[c]) == cudaSuccess) p = c;
+    }
+    if (p < 0) p = s->res_rr % kResStreams;
+    s->res_rr = p + 1;
+    const cudaStream_t ps = s->res_pool[p];
+    S_TRY(cudaStreamWaitEvent(ps, s->res_ready, 0), "cudaStreamWaitEvent");
+    for (size_t i = b; i < e; ++i)
+      S_TRY(cudaStreamWaitEvent(ps, list[i]->ev_in, 0),
+            "cudaStreamWaitEvent");
     const int cl = list[b]->r_cluster, v = list[b]->r_variant;
     const int nclusters =
         std::min<int>((int)(e - b), res_max_clusters(s, v, cl, smem));
     S_TRY(d3d::launch_resident(v, st.d + b, (int)(e - b), st.d_queue + ci,
-                               st.d_steps, cl, nclusters, smem, rs),
+                               st.d_steps, cl, nclusters, smem, ps),
           "resident launch");
     ++s->res_launches;
     ++s->launches;
     d3d::note_launches(1);
+    // The results go out on the launch's own stream: the shared copy
+    // stream carries the inputs of later admissions, which must not wait
+    // for these launches.
+    for (size_t i = b; i < e; ++i) {
+      Request* r = list[i];
+      S_TRY(cudaMemcpyAsync(r->host_out, s->arena + r->off_a,
+                            dense_bytes(r), cudaMemcpyDeviceToHost, ps),
+            "D2H copy (result)");
+      S_TRY(cudaEventCreateWithFlags(&r->ev_out, cudaEventDisableTiming),
+            "cudaEventCreate");
+      S_TRY(cudaEventRecord(r->ev_out, ps), "cudaEventRecord");
+      s->retiring.push_back(r);
+      ++s->res_solves;
+    }
+    S_TRY(cudaEventRecord(s->res_join[p], ps), "cudaEventRecord");
+    S_TRY(cudaStreamWaitEvent(gs, s->res_join[p], 0), "cudaStreamWaitEvent");
     b = e;
   }
-  S_TRY(cudaEventRecord(st.done, rs), "cudaEventRecord");
+  S_TRY(cudaEventRecord(st.done, gs), "cudaEventRecord");
   st.in_flight = true;
-  // The results go out on the resident stream itself: the shared copy
-  // stream carries the inputs of later admissions, which must not wait for
-  // this group's launches.
-  for (Request* r : list) {
-    S_TRY(cudaMemcpyAsync(r->host_out, s->arena + r->off_a, dense_bytes(r),
-                          cudaMemcpyDeviceToHost, rs),
-          "D2H copy (result)");
-    S_TRY(cudaEventCreateWithFlags(&r->ev_out, cudaEventDisableTiming),
-          "cudaEventCreate");
-    S_TRY(cudaEventRecord(r->ev_out, rs), "cudaEventRecord");
-    s->retiring.push_back(r);
-    ++s->res_solves;
-  }
-  list.clear();
+  list.erase(list.begin(), list.begin() + n);
   return D3D_OK;
 }
 
@@ -548,7 +554,7 @@ constexpr long kSlabTarget = 8 * 148;
 constexpr int kMaxSlab = 32, kMinSlab = 16;
 // Steps per tick: chunk * clamp(ceil(remaining / (chunk * kStepHorizon)),
 // 1, kMaxStepMult).
-constexpr int kStepHorizon = 8, kMaxStepMult = 4;
+constexpr int kStepHorizon = 4, kMaxStepMult = 4;
 int slab_planes(int nz, int cap) {
   const int ns = (nz + cap - 1) / cap;
   return (nz + ns - 1) / ns;  // balanced slabs of at most `cap` planes
@@ -792,8 +798,6 @@ int d3d_server_create(size_t arena_bytes, int chunk, d3d_server* out) {
     e = cudaStreamCreateWithFlags(&s->lane[l], cudaStreamNonBlocking);
   if (e == cudaSuccess)
     e = cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking);
-  if (e == cudaSuccess)
-    e = cudaStreamCreateWithFlags(&s->res_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     d3d_server_destroy(s);
     return d3d::set_cuda_error(e, "server setup");
@@ -878,6 +882,38 @@ int d3d_server_set_resident(d3d_server s, int on) {
       !s->res_pending.empty())
     return sfail(D3D_E_BUSY,
                  "the resident path changes only on an idle server");
+  if (on && !s->res_ready) {
+    for (int i = 0; i < kResStreams; ++i) {
+      S_TRY(cudaStreamCreateWithFlags(&s->res_pool[i],
+                                      cudaStreamNonBlocking),
+            "cudaStreamCreate");
+      S_TRY(cudaEventCreateWithFlags(&s->res_join[i],
+                                     cudaEventDisableTiming),
+            "cudaEventCreate");
+    }
+    S_TRY(cudaEventCreateWithFlags(&s->res_ready, cudaEventDisableTiming),
+          "cudaEventCreate");
+  }
+  if (on && s->rstage.empty()) {
+    for (int i = 0; i < kResStages; ++i) {
+      ResStaging* st = new (std::nothrow) ResStaging();
+      if (!st) return sfail(D3D_E_OOM, "resident staging");
+      s->rstage.push_back(st);  // freed by d3d_server_destroy
+      st->cap = kResGroupCap;
+      S_TRY(cudaMallocHost(&st->h, st->cap * sizeof(d3d::ResidentDesc)),
+            "cudaMallocHost (resident staging)");
+      S_TRY(cudaMalloc(&st->d, st->cap * sizeof(d3d::ResidentDesc)),
+            "cudaMalloc (resident staging)");
+      S_TRY(cudaMalloc(&st->d_steps, st->cap * sizeof(int)),
+            "cudaMalloc (resident step counters)");
+      S_TRY(cudaMalloc(&st->d_queue, kMaxResClasses * sizeof(unsigned)),
+            "cudaMalloc (resident work counters)");
+      S_TRY(cudaEventCreateWithFlags(&st->done, cudaEventDisableTiming),
+            "cudaEventCreate");
+      S_TRY(cudaStreamCreateWithFlags(&st->stream, cudaStreamNonBlocking),
+            "cudaStreamCreate");
+    }
+  }
   s->resident = on != 0;
   return D3D_OK;
 }
@@ -947,7 +983,10 @@ int d3d_server_destroy(d3d_server s) {
   if (!s) return D3D_OK;
   for (cudaStream_t l : s->lane)
     if (l) cudaStreamSynchronize(l);
-  if (s->res_stream) cudaStreamSynchronize(s->res_stream);
+  for (cudaStream_t p : s->res_pool)
+    if (p) cudaStreamSynchronize(p);
+  for (ResStaging* st : s->rstage)
+    if (st->stream) cudaStreamSynchronize(st->stream);
   if (s->copy) cudaStreamSynchronize(s->copy);
   for (Request* r : s->queued) delete r;
   for (Request* r : s->active) free_request(s, r);
@@ -959,9 +998,14 @@ int d3d_server_destroy(d3d_server s) {
     if (st->d_steps) cudaFree(st->d_steps);
     if (st->d_queue) cudaFree(st->d_queue);
     if (st->done) cudaEventDestroy(st->done);
+    if (st->stream) cudaStreamDestroy(st->stream);
     delete st;
   }
-  if (s->res_stream) cudaStreamDestroy(s->res_stream);
+  for (int i = 0; i < kResStreams; ++i) {
+    if (s->res_pool[i]) cudaStreamDestroy(s->res_pool[i]);
+    if (s->res_join[i]) cudaEventDestroy(s->res_join[i]);
+  }
+  if (s->res_ready) cudaEventDestroy(s->res_ready);
   for (auto& st : s->stage) {
     if (st.h_desc) cudaFreeHost(st.h_desc);
     if (st.h_items) cudaFreeHost(st.h_items);
