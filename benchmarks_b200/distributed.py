@@ -152,18 +152,26 @@ def exchange(dist, field, dec, group=None):
 class SlabSolver:
     """Runs `count` steps of one global field split across the group.
 
-    Two schedules, both bit-identical to a one-GPU run:
-    * overlap=True (halo 1): every step first computes the two owned planes
+    Three schedules, all bit-identical to a one-GPU run:
+    * overlap=True, halo 1: every step first computes the two owned planes
       the neighbours need (d3d_step_planes), posts their exchange into the
       neighbours' ghost planes of the output buffer, computes the interior
       planes while the planes travel, then waits.  No plane is computed
       twice.
+    * overlap=True, halo k >= 2 (passes of k steps): each pass first runs
+      k steps on a 3k-plane piece around every rank boundary ([lo-k, lo+2k)
+      below, [hi-2k, hi+k) above, on copies), whose middle k planes are
+      then exact; they go to the neighbour while the owned planes [lo, hi)
+      run k steps in one call (the plan's kernels: fused two-step passes
+      where it uses them), exact except the k planes at each rank
+      boundary, which the pieces' planes overwrite.  The received planes
+      land in side buffers and become the next pass's ghosts.  The pieces
+      cost 2k extra planes of stepping per boundary; a pass exchanges once.
     * overlap=False (halo h >= 1): every h steps the ranks exchange their h
       outermost owned planes, then each rank runs h steps on its whole
-      local buffer with one RunKernel-style call (the plan's kernels: fused
-      two-step passes where it uses them); the ghost planes are computed
-      redundantly and go stale one plane per step, never reaching an owned
-      plane within h steps.
+      local buffer with one RunKernel-style call; the ghost planes are
+      computed redundantly and go stale one plane per step, never reaching
+      an owned plane within h steps.
 
     step_fn(src, dst), when given, replaces the CUDA plan (one whole-buffer
     step; overlap is then unavailable): the CPU tests pass the oracle's
@@ -174,12 +182,17 @@ class SlabSolver:
                  device=None, dtype=None, overlap=False):
         import torch
         self.dist = dist
-        if overlap and (halo != 1 or step_fn is not None):
-            raise ValueError("the overlapped schedule is halo 1 on the "
+        if overlap and halo == 1 and step_fn is not None:
+            raise ValueError("the halo-1 overlapped schedule runs on the "
                              "CUDA plan")
         self.overlap = overlap
         self.dec = SlabDecomposition(nz, dist.get_rank(),
                                      dist.get_world_size(), halo)
+        d = self.dec
+        if (overlap and halo > 1 and (d.down is not None or d.up is not None)
+                and d.z1 - d.z0 < 2 * halo):
+            raise ValueError("the overlapped schedule needs at least "
+                             "2 x halo owned planes a rank")
         self.nx, self.ny, self.nz = nx, ny, nz
         self.coeff = np.ascontiguousarray(coeff)
         self.device = device if device is not None else torch.device("cuda")
@@ -188,11 +201,28 @@ class SlabSolver:
         self.f1 = torch.zeros(shape, dtype=self.dtype, device=self.device)
         self.f2 = torch.zeros_like(self.f1)
         self._plan = None
+        self._plan_own = self._plan_piece = None
+        self.step_fn = step_fn
         if step_fn is None:
             from . import F32, F64, Plan
-            self._plan = Plan(nx, ny, self.dec.local_nz,
-                              F64 if self.dtype == torch.float64 else F32)
-        self.step_fn = step_fn
+            dt = F64 if self.dtype == torch.float64 else F32
+            self._plan = Plan(nx, ny, d.local_nz, dt)
+            if overlap and halo > 1:
+                self._plan_own = Plan(nx, ny, d.z1 - d.z0, dt)
+                if d.down is not None or d.up is not None:
+                    self._plan_piece = Plan(nx, ny, 3 * halo, dt)
+        if overlap and halo > 1:
+            # per neighbour: the piece's two buffers and the ghost landing
+            self._pieces = {}
+            for side in ("down", "up"):
+                if getattr(d, side) is not None:
+                    self._pieces[side] = (
+                        torch.empty((3 * halo, ny, nx), dtype=self.dtype,
+                                    device=self.device),
+                        torch.empty((3 * halo, ny, nx), dtype=self.dtype,
+                                    device=self.device),
+                        torch.empty((halo, ny, nx), dtype=self.dtype,
+                                    device=self.device))
 
     def load(self, global_field):
         """Copies this rank's planes (with ghosts) of a global field."""
@@ -229,7 +259,59 @@ class SlabSolver:
         xchg.wait()
         self.f1, self.f2 = f2, f1
 
+    def _steps(self, plan, a, b, k):
+        """k steps ping-ponging (a, b) on `plan` (or step_fn); returns the
+        buffer holding the result."""
+        if plan is not None:
+            return plan.run(a, b, k, self.coeff)[0]
+        for _ in range(k):
+            self.step_fn(a, b)
+            a, b = b, a
+        return a
+
+    def _pass_fused(self, k):
+        """One k-step pass of the halo-k overlapped schedule (k <= halo)."""
+        d, h = self.dec, self.dec.halo
+        f1, f2 = self.f1, self.f2
+        lo, hi = d.z0 - d.lo, d.z1 - d.lo  # owned planes, local indices
+        first = {"down": lo - h, "up": hi - 2 * h}
+        peer = {"down": d.down, "up": d.up}
+        exact = {}
+        sends, recvs = [], []
+        for side, (pa, pb, ghost) in self._pieces.items():
+            pa.copy_(f1[first[side]:first[side] + 3 * h])
+            r = self._steps(self._plan_piece, pa, pb, k)
+            exact[side] = r[h:2 * h]   # exact after k <= h steps
+            sends.append((peer[side], exact[side]))
+            recvs.append((peer[side], ghost))
+        if any(_host_staged(self.dist, t) for _, t in sends):
+            import torch
+            torch.cuda.synchronize(self.device)
+        xchg = _Exchange(self.dist, sends, recvs)
+        own = self._steps(self._plan_own, f1[lo:hi], f2[lo:hi], k)
+        res, other = (f1, f2) if own.data_ptr() == f1[lo:hi].data_ptr() \
+            else (f2, f1)
+        if "down" in exact:
+            res[lo:lo + h].copy_(exact["down"])
+        if "up" in exact:
+            res[hi - h:hi].copy_(exact["up"])
+        xchg.wait()
+        if "down" in self._pieces:
+            res[lo - h:lo].copy_(self._pieces["down"][2])
+        if "up" in self._pieces:
+            res[hi:hi + h].copy_(self._pieces["up"][2])
+        self.f1, self.f2 = res, other
+
     def run(self, count):
+        if self.overlap and self.dec.halo > 1:
+            h, done = self.dec.halo, 0
+            if self._pieces:  # the first pass needs current ghosts
+                exchange(self.dist, self.f1, self.dec)
+            while done < count:
+                k = min(h, count - done)
+                self._pass_fused(k)
+                done += k
+            return self.f1[self.dec.owned()]
         if self.overlap:
             for _ in range(count):
                 self._step_overlapped()
@@ -266,6 +348,8 @@ class SlabSolver:
         return torch.cat([p[:z1 - z0] for p, (z0, z1) in zip(parts, sizes)])
 
     def close(self):
-        if self._plan is not None:
-            self._plan.close()
-            self._plan = None
+        for name in ("_plan", "_plan_own", "_plan_piece"):
+            plan = getattr(self, name, None)
+            if plan is not None:
+                plan.close()
+                setattr(self, name, None)

@@ -5,9 +5,10 @@
   single-process run, for several world sizes, halo depths and uneven
   slabs.
 * (GPU) the same with the CUDA kernels: 2 or 3 gloo ranks share one GPU,
-  each stepping its slab through the C ABI (the overlapped schedule with
-  d3d_step_planes, and the halo-h schedule with whole-buffer runs), the
-  planes staged through host memory; no kernel waits on another rank's.
+  each stepping its slab through the C ABI (the halo-1 overlapped schedule
+  with d3d_step_planes, the overlapped schedule of k-step passes, and the
+  halo-h schedule with whole-buffer runs), the planes staged through host
+  memory; no kernel waits on another rank's.
 * bench-style max-over-ranks timing reduction.
 """
 import os
@@ -52,7 +53,8 @@ def _free_port():
     return port
 
 
-def _slab_worker(rank, world, port, nx, ny, nz, count, halo, seed, out):
+def _slab_worker(rank, world, port, nx, ny, nz, count, halo, seed, out,
+                 overlap=False):
     import torch
     import torch.distributed as dist
     from datetime import timedelta
@@ -77,7 +79,7 @@ def _slab_worker(rank, world, port, nx, ny, nz, count, halo, seed, out):
                               c.ctypes.data_as(O._f32p))
 
         solver = SlabSolver(dist, nx, ny, nz, c, halo=halo, step_fn=step,
-                            device=torch.device("cpu"))
+                            device=torch.device("cpu"), overlap=overlap)
         solver.load(torch.from_numpy(field))
         solver.run(count)
         full = solver.gather().numpy()
@@ -91,14 +93,19 @@ def _slab_worker(rank, world, port, nx, ny, nz, count, halo, seed, out):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world,halo,dims,count", [
-    (2, 1, (12, 9, 16), 7),
-    (2, 3, (10, 7, 15), 8),
-    (3, 2, (8, 8, 17), 11),
-    (3, 1, (5, 6, 7), 5),
+@pytest.mark.parametrize("world,halo,overlap,dims,count", [
+    (2, 1, False, (12, 9, 16), 7),
+    (2, 3, False, (10, 7, 15), 8),
+    (3, 2, False, (8, 8, 17), 11),
+    (3, 1, False, (5, 6, 7), 5),
+    # the overlapped schedule of k-step passes (pieces around each rank
+    # boundary first), with a shorter last pass when count % halo != 0
+    (2, 2, True, (12, 9, 16), 7),
+    (3, 3, True, (10, 7, 20), 8),
+    (4, 2, True, (6, 5, 19), 9),
 ])
-def test_slab_solver_matches_single_process(tmp_path, world, halo, dims,
-                                            count):
+def test_slab_solver_matches_single_process(tmp_path, world, halo, overlap,
+                                            dims, count):
     import torch.multiprocessing as mp
 
     import oracle as O
@@ -106,7 +113,7 @@ def test_slab_solver_matches_single_process(tmp_path, world, halo, dims,
     out = str(tmp_path / "full.npy")
     mp.start_processes(_slab_worker,
                        args=(world, _free_port(), nx, ny, nz, count, halo, 5,
-                             out),
+                             out, overlap),
                        nprocs=world, join=True, start_method="spawn")
     full = np.load(out)
     c, _ = O.params(nx, ny, nz)
@@ -149,6 +156,9 @@ def _slab_cuda_worker(rank, world, port, nx, ny, nz, count, halo, overlap,
     (3, 1, True, (136, 17, 23), 6),
     (2, 2, False, (64, 40, 36), 9),
     (2, 3, False, (130, 24, 31), 7),
+    (2, 2, True, (128, 40, 36), 9),
+    (3, 2, True, (136, 17, 23), 6),
+    (2, 3, True, (130, 24, 31), 7),
 ])
 def test_slab_solver_cuda_kernels_across_ranks(tmp_path, world, halo, overlap,
                                                dims, count):
@@ -223,7 +233,7 @@ def test_slab_solver_cuda_kernels_world_one():
                             timeout=timedelta(seconds=60))
     try:
         fulls = []
-        for halo, overlap in ((2, False), (1, True)):
+        for halo, overlap in ((2, False), (1, True), (2, True)):
             solver = SlabSolver(dist, nx, ny, nz, c, halo=halo,
                                 overlap=overlap)
             solver.load(torch.from_numpy(field).cuda())
