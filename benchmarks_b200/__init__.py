@@ -24,6 +24,7 @@ HEADER = os.path.join(ROOT, "include", "d3d_b200.h")
 D3D_OK = 0
 D3D_E_INVALID, D3D_E_CUDA, D3D_E_OOM = -1, -2, -3
 D3D_E_TIMEOUT, D3D_E_UNSUPPORTED, D3D_E_BUSY, D3D_E_IO = -4, -5, -6, -7
+D3D_E_TRANSPORT = -8
 F32, F64 = 0, 1
 KERNEL_AUTO, KERNEL_GENERIC, KERNEL_TMA, KERNEL_TB = 0, 1, 2, 3
 NUM_TILE_VARIANTS = 6
@@ -58,6 +59,10 @@ _SIGNATURES = {
     "d3d_step": ([_vp, _vp, _vp, _vp, _vp], _i),
     "d3d_step_planes": ([_vp, _vp, _vp, _i, _i, _vp, _vp], _i),
     "d3d_run": ([_vp, _vpp, _vpp, _vp, _i, _vp], _i),
+    "d3d_slab_create": ([_i, _i, _i, _i, _i, _i, _i, _vpp,
+                         ctypes.POINTER(ctypes.c_int)], _i),
+    "d3d_slab_run": ([_vp, _vpp, _vpp, _vp, _i, _vp, _vp], _i),
+    "d3d_slab_destroy": ([_vp], _i),
     "d3d_run_host": ([_vp, _vp, _vp, _vp, _vp, _i, _vp,
                       ctypes.POINTER(ctypes.c_float)], _i),
     "d3d_analytic": ([_vp, _vp, ctypes.c_double, _vp], _i),

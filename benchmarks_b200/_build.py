@@ -39,7 +39,7 @@ NVCC_FLAGS = ARCH + [
 
 SOURCES = ["d3d_step.cu", "d3d_step2d.cu", "d3d_tb.cu", "d3d_tb2.cu",
            "d3d_norm.cu",
-           "d3d_batch.cu", "d3d_pitched.cu", "d3d_resident.cu", "d3d_serve.cu", "d3d_io.cu", "d3d_api.cu"]
+           "d3d_batch.cu", "d3d_pitched.cu", "d3d_resident.cu", "d3d_serve.cu", "d3d_io.cu", "d3d_slab.cu", "d3d_api.cu"]
 HEADERS = ["d3d_common.cuh", "d3d_kernels.h", "d3d_march.cuh"]
 
 

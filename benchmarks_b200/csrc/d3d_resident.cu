@@ -71,12 +71,6 @@ __device__ __forceinline__ unsigned cluster_rank() {
   return r;
 }
 
-__device__ __forceinline__ unsigned cluster_size() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
-  return r;
-}
-
 // The shared::cluster address of `cta_addr` (a shared::cta address) in CTA
 // `rank` of this cluster.
 __device__ __forceinline__ uint32_t map_to_rank(uint32_t cta_addr,

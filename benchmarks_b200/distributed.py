@@ -21,6 +21,8 @@ rank boundary.
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 
 
@@ -149,6 +151,80 @@ def exchange(dist, field, dec, group=None):
     _Exchange(dist, sends, recvs, group).wait()
 
 
+class _CudaArray:
+    """Device memory the library owns, seen through the CUDA array
+    interface so torch can wrap it without a copy."""
+
+    def __init__(self, ptr, count, typestr):
+        self.__cuda_array_interface__ = {
+            "shape": (count,), "typestr": typestr, "data": (ptr, False),
+            "version": 2}
+
+
+class _SlabTransport:
+    """d3d_slab_transport over a torch.distributed group: post() starts
+    the send/recv of the planes the library names (_Exchange: NCCL into
+    the receiver's memory, or host staging on gloo), wait() finishes it.
+    A Python exception in a callback is kept and re-raised by the caller
+    once the library has returned D3D_E_TRANSPORT."""
+
+    POST = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p,
+                            ctypes.POINTER(ctypes.c_void_p),
+                            ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t,
+                            ctypes.c_void_p)
+    WAIT = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p)
+
+    class Struct(ctypes.Structure):
+        _fields_ = [("post", ctypes.c_void_p), ("wait", ctypes.c_void_p),
+                    ("user", ctypes.c_void_p)]
+
+    def __init__(self, dist, dec, device, dtype):
+        import torch
+        self.dist, self.dec, self.device = dist, dec, device
+        self.dtype = dtype
+        self.esize = 8 if dtype == torch.float64 else 4
+        self.typestr = "<f8" if dtype == torch.float64 else "<f4"
+        self.error = None
+        self._xchg = None
+        self._post = self.POST(self._on_post)  # kept alive with the struct
+        self._wait = self.WAIT(self._on_wait)
+        self.struct = self.Struct(
+            ctypes.cast(self._post, ctypes.c_void_p),
+            ctypes.cast(self._wait, ctypes.c_void_p), None)
+
+    def _view(self, ptr, nbytes):
+        import torch
+        return torch.as_tensor(
+            _CudaArray(ptr, nbytes // self.esize, self.typestr),
+            device=self.device)
+
+    def _on_post(self, user, send, recv, nbytes, stream):
+        try:
+            peers = (self.dec.down, self.dec.up)
+            sends, recvs = [], []
+            for i in range(2):
+                if send[i]:
+                    sends.append((peers[i], self._view(send[i], nbytes)))
+                    recvs.append((peers[i], self._view(recv[i], nbytes)))
+            if any(_host_staged(self.dist, t) for _, t in sends):
+                import torch
+                torch.cuda.synchronize(self.device)
+            self._xchg = _Exchange(self.dist, sends, recvs)
+            return 0
+        except BaseException as e:  # reported through the return code
+            self.error = e
+            return 1
+
+    def _on_wait(self, user, stream):
+        try:
+            xchg, self._xchg = self._xchg, None
+            xchg.wait()
+            return 0
+        except BaseException as e:
+            self.error = e
+            return 1
+
+
 class SlabSolver:
     """Runs `count` steps of one global field split across the group.
 
@@ -158,15 +234,17 @@ class SlabSolver:
       neighbours' ghost planes of the output buffer, computes the interior
       planes while the planes travel, then waits.  No plane is computed
       twice.
-    * overlap=True, halo k >= 2 (passes of k steps): each pass first runs
-      k steps on a 3k-plane piece around every rank boundary ([lo-k, lo+2k)
-      below, [hi-2k, hi+k) above, on copies), whose middle k planes are
-      then exact; they go to the neighbour while the owned planes [lo, hi)
-      run k steps in one call (the plan's kernels: fused two-step passes
-      where it uses them), exact except the k planes at each rank
-      boundary, which the pieces' planes overwrite.  The received planes
-      land in side buffers and become the next pass's ghosts.  The pieces
-      cost 2k extra planes of stepping per boundary; a pass exchanges once.
+    * overlap=True, halo k >= 2 (passes of k steps; d3d_slab_run, the
+      pass loop in the library, with this group's send/recv as its
+      transport): each pass first runs k steps on a 3k-plane piece around
+      every rank boundary ([lo-k, lo+2k) below, [hi-2k, hi+k) above, on
+      copies), whose middle k planes are then exact; they go to the
+      neighbour while the owned planes [lo, hi) run k steps in one call
+      (the plan's kernels: fused two-step passes where it uses them), exact
+      except the k planes at each rank boundary, which the pieces' planes
+      overwrite.  The received planes land in side buffers and become the
+      next pass's ghosts.  The pieces cost 2k extra planes of stepping per
+      boundary; a pass exchanges once.
     * overlap=False (halo h >= 1): every h steps the ranks exchange their h
       outermost owned planes, then each rank runs h steps on its whole
       local buffer with one RunKernel-style call; the ghost planes are
@@ -201,19 +279,28 @@ class SlabSolver:
         self.f1 = torch.zeros(shape, dtype=self.dtype, device=self.device)
         self.f2 = torch.zeros_like(self.f1)
         self._plan = None
-        self._plan_own = self._plan_piece = None
+        self._slab = None          # the C-ABI slab (CUDA, overlapped passes)
+        self._transport = None
+        self._pieces = {}          # the same schedule for a step_fn
         self.step_fn = step_fn
+        neighbours = d.down is not None or d.up is not None
         if step_fn is None:
-            from . import F32, F64, Plan
+            from . import F32, F64, Plan, check, lib
             dt = F64 if self.dtype == torch.float64 else F32
-            self._plan = Plan(nx, ny, d.local_nz, dt)
             if overlap and halo > 1:
-                self._plan_own = Plan(nx, ny, d.z1 - d.z0, dt)
-                if d.down is not None or d.up is not None:
-                    self._plan_piece = Plan(nx, ny, 3 * halo, dt)
-        if overlap and halo > 1:
+                self._slab = ctypes.c_void_p()
+                lnz = ctypes.c_int()
+                check(lib().d3d_slab_create(nx, ny, nz, d.z0, d.z1, halo, dt,
+                                            ctypes.byref(self._slab),
+                                            ctypes.byref(lnz)))
+                assert lnz.value == d.local_nz
+                if neighbours:
+                    self._transport = _SlabTransport(dist, d, self.device,
+                                                     self.dtype)
+            else:
+                self._plan = Plan(nx, ny, d.local_nz, dt)
+        elif overlap and halo > 1:
             # per neighbour: the piece's two buffers and the ghost landing
-            self._pieces = {}
             for side in ("down", "up"):
                 if getattr(d, side) is not None:
                     self._pieces[side] = (
@@ -259,18 +346,18 @@ class SlabSolver:
         xchg.wait()
         self.f1, self.f2 = f2, f1
 
-    def _steps(self, plan, a, b, k):
-        """k steps ping-ponging (a, b) on `plan` (or step_fn); returns the
-        buffer holding the result."""
-        if plan is not None:
-            return plan.run(a, b, k, self.coeff)[0]
+    def _steps(self, a, b, k):
+        """k steps of step_fn ping-ponging (a, b); returns the buffer
+        holding the result."""
         for _ in range(k):
             self.step_fn(a, b)
             a, b = b, a
         return a
 
     def _pass_fused(self, k):
-        """One k-step pass of the halo-k overlapped schedule (k <= halo)."""
+        """One k-step pass (k <= halo) of the overlapped-pass schedule on
+        step_fn: the pass loop of d3d_slab_run, written out for the host
+        tests (the CUDA path runs it in the library)."""
         d, h = self.dec, self.dec.halo
         f1, f2 = self.f1, self.f2
         lo, hi = d.z0 - d.lo, d.z1 - d.lo  # owned planes, local indices
@@ -280,15 +367,12 @@ class SlabSolver:
         sends, recvs = [], []
         for side, (pa, pb, ghost) in self._pieces.items():
             pa.copy_(f1[first[side]:first[side] + 3 * h])
-            r = self._steps(self._plan_piece, pa, pb, k)
+            r = self._steps(pa, pb, k)
             exact[side] = r[h:2 * h]   # exact after k <= h steps
             sends.append((peer[side], exact[side]))
             recvs.append((peer[side], ghost))
-        if any(_host_staged(self.dist, t) for _, t in sends):
-            import torch
-            torch.cuda.synchronize(self.device)
         xchg = _Exchange(self.dist, sends, recvs)
-        own = self._steps(self._plan_own, f1[lo:hi], f2[lo:hi], k)
+        own = self._steps(f1[lo:hi], f2[lo:hi], k)
         res, other = (f1, f2) if own.data_ptr() == f1[lo:hi].data_ptr() \
             else (f2, f1)
         if "down" in exact:
@@ -302,16 +386,40 @@ class SlabSolver:
             res[hi:hi + h].copy_(self._pieces["up"][2])
         self.f1, self.f2 = res, other
 
+    def _run_slab(self, count):
+        """`count` steps through d3d_slab_run (the pass loop in the
+        library; this group's send/recv as its transport)."""
+        import torch
+        from . import D3D_E_TRANSPORT, check, lib
+        a = ctypes.c_void_p(self.f1.data_ptr())
+        b = ctypes.c_void_p(self.f2.data_ptr())
+        t = self._transport
+        rc = lib().d3d_slab_run(
+            self._slab, ctypes.byref(a), ctypes.byref(b),
+            self.coeff.ctypes.data, count,
+            ctypes.byref(t.struct) if t is not None else None,
+            torch.cuda.current_stream(self.device).cuda_stream)
+        if rc == D3D_E_TRANSPORT and t is not None and t.error is not None:
+            err, t.error = t.error, None
+            raise err
+        check(rc)
+        if a.value != self.f1.data_ptr():
+            self.f1, self.f2 = self.f2, self.f1
+
     def run(self, count):
         if self.overlap and self.dec.halo > 1:
-            h, done = self.dec.halo, 0
-            if self._pieces:  # the first pass needs current ghosts
-                exchange(self.dist, self.f1, self.dec)
-            while done < count:
-                k = min(h, count - done)
-                self._pass_fused(k)
-                done += k
-            return self.f1[self.dec.owned()]
+            d = self.dec
+            if d.down is not None or d.up is not None:
+                exchange(self.dist, self.f1, d)  # current ghosts to start
+            if self._slab is not None:
+                self._run_slab(count)
+            else:
+                h, done = d.halo, 0
+                while done < count:
+                    k = min(h, count - done)
+                    self._pass_fused(k)
+                    done += k
+            return self.f1[d.owned()]
         if self.overlap:
             for _ in range(count):
                 self._step_overlapped()
@@ -348,8 +456,10 @@ class SlabSolver:
         return torch.cat([p[:z1 - z0] for p, (z0, z1) in zip(parts, sizes)])
 
     def close(self):
-        for name in ("_plan", "_plan_own", "_plan_piece"):
-            plan = getattr(self, name, None)
-            if plan is not None:
-                plan.close()
-                setattr(self, name, None)
+        if self._plan is not None:
+            self._plan.close()
+            self._plan = None
+        if self._slab is not None:
+            from . import lib
+            lib().d3d_slab_destroy(self._slab)
+            self._slab = None

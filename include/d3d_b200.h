@@ -38,8 +38,9 @@ enum {
   D3D_E_TIMEOUT = -4,     /* a bounded device wait ran out */
   D3D_E_UNSUPPORTED = -5, /* shape/dtype/kernel combination not supported */
   D3D_E_BUSY = -6,        /* admission refused (serving) */
-  D3D_E_IO = -7           /* a checkpoint file could not be written or read,
+  D3D_E_IO = -7,          /* a checkpoint file could not be written or read,
                              or failed its checksum */
+  D3D_E_TRANSPORT = -8    /* a z-slab transport callback reported failure */
 };
 
 enum { D3D_F32 = 0, D3D_F64 = 1 };
@@ -171,6 +172,62 @@ int d3d_step_planes(d3d_plan plan, const void* f1, void* f2, int z_begin,
  * single steps finish the job (exactly `count` steps for any count). */
 int d3d_run(d3d_plan plan, void** f1, void** f2, const void* coeff, int count,
             void* stream);
+
+/* ---------------------------------------------------------------------
+ * One rank's z slab of a global nx*ny*nz grid split across processes (no
+ * counterpart in the reference, whose only multi-node path is the external
+ * Physis MPI runtime, src/diffusion3d/Makefile:253-268).  The rank owns
+ * planes [z0, z1) and holds `halo` ghost planes on each side that has a
+ * neighbour: a local buffer of planes [max(z0-halo, 0), min(z1+halo, nz)).
+ * d3d_slab_run advances it in passes of k <= halo steps:
+ *   1. for each neighbour, k steps of a 3*halo-plane piece around the rank
+ *      boundary (copied out of the field), whose middle halo planes are
+ *      then exact (a step clamped at a false edge is wrong only next to
+ *      it, one more plane per step);
+ *   2. transport.post hands those planes to the neighbours and names where
+ *      theirs land;
+ *   3. k steps of the owned planes in one d3d_run (fused two-step passes
+ *      where the plan uses them), exact except the halo planes at each
+ *      rank boundary, which step 1's planes overwrite;
+ *   4. transport.wait, then the received planes become the ghosts.
+ * The owned planes stay bit-identical to a one-GPU run of the whole grid.
+ * ------------------------------------------------------------------- */
+typedef struct d3d_slab_s* d3d_slab;
+
+typedef struct d3d_slab_transport {
+  /* Starts this pass's exchange: send[i] -> the neighbour on side i (0: the
+   * rank below, owning lower z; 1: the rank above) and that neighbour's
+   * planes into recv[i]; `bytes` each, device memory; NULL entries for a
+   * side without a neighbour.  send[i] is ready once the work queued on
+   * `stream` so far has run and stays untouched until wait() returns;
+   * recv[i] is not read before wait() returns.  Nonzero: failure. */
+  int (*post)(void* user, void* const send[2], void* const recv[2],
+              size_t bytes, void* stream);
+  /* Returns once work queued on `stream` after it is ordered after the
+   * receives (or once they have landed).  Nonzero: failure. */
+  int (*wait)(void* user, void* stream);
+  void* user;
+} d3d_slab_transport;
+
+/* Creates the slab state for owned planes [z0, z1) of an nx*ny*nz grid
+ * (0 <= z0 < z1 <= nz, halo >= 1; with a neighbour, z1 - z0 >= 2*halo and
+ * halo planes beyond that side).  It owns two plans and, per neighbour,
+ * two 3*halo-plane piece buffers and one halo-plane landing buffer; the
+ * field's buffers are the caller's.  *local_nz (may be NULL) receives the
+ * planes of the caller's buffers. */
+int d3d_slab_create(int nx, int ny, int nz, int z0, int z1, int halo,
+                    int dtype, d3d_slab* out, int* local_nz);
+
+/* `count` steps of the slab held in *f1 (local_nz planes, ghost planes
+ * current), ping-ponging with *f2; on return *f1 holds the result, its
+ * ghost planes current, like d3d_run.  `transport` may be NULL only
+ * without neighbours.  A callback's failure ends the run with
+ * D3D_E_TRANSPORT after its queued work. */
+int d3d_slab_run(d3d_slab slab, void** f1, void** f2, const void* coeff,
+                 int count, const d3d_slab_transport* transport,
+                 void* stream);
+
+int d3d_slab_destroy(d3d_slab slab);
 
 /* Diffusion3DCUDA::RunKernel(count) as a whole (diffusion3d_cuda.cu:353-371):
  * copies host_f1 to dev_f1, runs `count` steps between dev_f1 and dev_f2,

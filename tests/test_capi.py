@@ -58,6 +58,31 @@ def test_plan_create_rejects_bad_arguments():
     assert L.d3d_run(None, None, None, None, 1, None) == B.D3D_E_INVALID
 
 
+def test_slab_create_rejects_bad_geometry():
+    """d3d_slab_create checks its geometry before any device work."""
+    h = ctypes.c_void_p()
+    L = B.lib()
+    bad = [
+        (0, 4, 16, 0, 8, 1),     # nx < 1
+        (4, 4, 16, 8, 8, 1),     # empty slab
+        (4, 4, 16, 0, 17, 1),    # past the grid
+        (4, 4, 16, 0, 8, 0),     # halo < 1
+        (4, 4, 16, 1, 9, 2),     # the rank below holds 1 plane < halo
+        (4, 4, 16, 8, 15, 2),    # the rank above holds 1 plane < halo
+        (4, 4, 16, 4, 7, 2),     # 3 owned planes < 2 x halo with neighbours
+    ]
+    for nx, ny, nz, z0, z1, halo in bad:
+        assert L.d3d_slab_create(nx, ny, nz, z0, z1, halo, B.F32,
+                                 ctypes.byref(h), None) == B.D3D_E_INVALID
+    assert L.d3d_slab_create(4, 4, 16, 0, 16, 1, 5, ctypes.byref(h),
+                             None) == B.D3D_E_INVALID       # dtype
+    assert L.d3d_slab_create(4, 4, 16, 0, 16, 1, B.F32, None,
+                             None) == B.D3D_E_INVALID       # no output
+    assert L.d3d_slab_run(None, None, None, None, 1, None, None) \
+        == B.D3D_E_INVALID
+    assert L.d3d_slab_destroy(None) == B.D3D_OK
+
+
 @pytest.mark.parametrize("nd,dims", [(2, (256, 256)), (2, (37, 23)),
                                      (2, (1, 1)), (3, (64, 64, 64)),
                                      (3, (17, 23, 5)), (3, (24, 40, 16))])

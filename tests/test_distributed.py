@@ -245,3 +245,61 @@ def test_slab_solver_cuda_kernels_world_one():
         dist.destroy_process_group()
     for full in fulls:
         assert full.tobytes() == O.run(field, c, count).tobytes()
+
+
+@pytest.mark.gpu
+def test_slab_transport_failure_is_reported():
+    """A transport callback that fails ends d3d_slab_run with
+    D3D_E_TRANSPORT after the work it queued; the Python exception comes
+    back to the caller, and the slab stays usable."""
+    import ctypes
+
+    import torch
+
+    import benchmarks_b200 as B
+    import oracle as O
+    from benchmarks_b200.distributed import SlabDecomposition, _SlabTransport
+
+    nx, ny, nz = 32, 16, 24
+    c, _ = O.params(nx, ny, nz)
+    dec = SlabDecomposition(nz, 1, 2, halo=2)   # owns [12, 24), one below
+
+    class Boom(RuntimeError):
+        pass
+
+    class Group:      # post() raises before any transfer
+        @staticmethod
+        def get_backend():
+            return "nccl"
+
+        @staticmethod
+        def batch_isend_irecv(ops):
+            raise Boom("no peer")
+
+        P2POp = staticmethod(lambda *a: a)
+        isend = irecv = None
+
+    slab = ctypes.c_void_p()
+    lnz = ctypes.c_int()
+    B.check(B.lib().d3d_slab_create(nx, ny, nz, dec.z0, dec.z1, 2, B.F32,
+                                    ctypes.byref(slab), ctypes.byref(lnz)))
+    try:
+        assert lnz.value == dec.local_nz == 14
+        f1 = torch.zeros((lnz.value, ny, nx), device="cuda")
+        f2 = torch.zeros_like(f1)
+        t = _SlabTransport(Group, dec, f1.device, torch.float32)
+        a = ctypes.c_void_p(f1.data_ptr())
+        b = ctypes.c_void_p(f2.data_ptr())
+        rc = B.lib().d3d_slab_run(slab, ctypes.byref(a), ctypes.byref(b),
+                                  c.ctypes.data, 2, ctypes.byref(t.struct),
+                                  torch.cuda.current_stream().cuda_stream)
+        assert rc == B.D3D_E_TRANSPORT
+        assert isinstance(t.error, Boom)
+        assert "transport" in B.lib().d3d_last_error().decode()
+        # a neighbour and no transport: refused before any launch
+        rc = B.lib().d3d_slab_run(slab, ctypes.byref(a), ctypes.byref(b),
+                                  c.ctypes.data, 2, None, None)
+        assert rc == B.D3D_E_INVALID
+        torch.cuda.synchronize()
+    finally:
+        B.lib().d3d_slab_destroy(slab)
