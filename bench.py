@@ -755,7 +755,7 @@ def main():
                     help="skip the CPU baseline leg")
     ap.add_argument("--no-side", action="store_true",
                     help="skip the batched, serving and 2D legs")
-    ap.add_argument("--only-leg", choices=["batched", "serving",
+    ap.add_argument("--only-leg", choices=["batched", "serving", "served",
                                            "diffusion2d", "slab"],
                     help="run one side leg alone on GPU 0 and print its "
                          "JSON (no headline line; for profiling)")
@@ -857,6 +857,8 @@ def run_one_leg(leg, batch_kind=None):
         out = batched_leg(B, torch, kind=batch_kind)
     elif leg == "serving":
         out = serving_leg(B, torch)
+    elif leg == "served":  # the server alone: no march or plain-loop runs
+        out = serving_leg(B, torch, compare=False)
     elif leg == "slab":
         out = slab_leg(B, torch, None)
     else:
