@@ -82,6 +82,7 @@ _SIGNATURES = {
     "d3d_copy_calibrate": ([_vp, _vp, _sz, ctypes.c_float, _i, _vp,
                             ctypes.POINTER(ctypes.c_float)], _i),
     "d3d_batch_set_kind": ([_vp, _i], _i),
+    "d3d_batch_set_resident_max_cluster": ([_vp, _i], _i),
     "d3d_batch_run": ([_vp, _vp, ctypes.POINTER(ctypes.c_float)], _i),
     "d3d_batch_info": ([_vp, ctypes.c_char_p, _sz], _i),
     "d3d_batch_progress": ([_vp, ctypes.POINTER(ctypes.c_int), _i], _i),
@@ -489,6 +490,11 @@ class Batch:
         its two-step form (grids at most 248 floats wide), 8 the
         cluster-resident kernel for every grid it fits."""
         check(lib().d3d_batch_set_kind(self._h, int(kind)))
+
+    def set_resident_max_cluster(self, n):
+        """Cluster-resident kernel only for grids that fit clusters of at
+        most n CTAs (1..16); 0 turns it off."""
+        check(lib().d3d_batch_set_resident_max_cluster(self._h, int(n)))
 
     def run(self, stream=None, timed=True):
         ms = ctypes.c_float()

@@ -179,6 +179,9 @@ struct d3d_batch_s {
   std::vector<int> rclass_of;            // per grid: index into rclasses
   std::vector<ResidentClass> rclasses;
   bool resident_on = false;
+  // Only classes of at most this many CTAs a cluster run resident; the
+  // larger grids keep the per-step kinds (the autotuner picks the bound).
+  int res_max_cluster = d3d::kResidentMaxCluster;
   int* d_counters = nullptr;
   int2* d_classic_steps = nullptr;  // (grid, steps) of the per-step grids
   int n_classic = 0;
@@ -554,6 +557,15 @@ void free_resident(d3d_batch b) {
 // Puts every grid (steps >= 0) into its size class, leaving out the grids
 // the cluster-resident kernel runs when it is on, and rebuilds the classes'
 // work lists and the repitch lists.
+bool runs_resident(const d3d_batch b, int i) {
+  return b->resident_on && b->resident_ok[i] &&
+         b->rclasses[b->rclass_of[i]].cluster <= b->res_max_cluster;
+}
+
+bool class_resident(const d3d_batch b, const ResidentClass& rc) {
+  return b->resident_on && rc.cluster <= b->res_max_cluster;
+}
+
 int assign_grids(d3d_batch b) {
   for (ClassPlan& c : b->cls) {
     c.grids.clear();
@@ -562,7 +574,7 @@ int assign_grids(d3d_batch b) {
   b->max_steps = 0;
   std::vector<int2> classic;
   for (int i = 0; i < (int)b->grids.size(); ++i) {
-    if (b->resident_on && b->resident_ok[i]) continue;
+    if (runs_resident(b, i)) continue;
     ClassPlan& c = b->cls[class_of(b->grids[i].nx)];
     c.grids.push_back(i);
     c.max_steps = std::max(c.max_steps, b->grids[i].steps);
@@ -598,9 +610,10 @@ int enqueue_all(d3d_batch b, cudaStream_t s, unsigned long long* launches) {
   bool used[kSideStreams] = {};
   if (b->resident_on && !b->rclasses.empty()) {
     B_TRY(cudaEventRecord(b->fork, s), "cudaEventRecord (fork)");
-    for (size_t ci = 0; ci < b->rclasses.size(); ++ci) {
+    for (size_t ci = 0, li = 0; ci < b->rclasses.size(); ++ci) {
       const ResidentClass& rc = b->rclasses[ci];
-      const int k = (int)(ci % kSideStreams);
+      if (!class_resident(b, rc)) continue;
+      const int k = (int)(li++ % kSideStreams);
       if (!used[k]) {
         B_TRY(cudaStreamWaitEvent(b->side[k], b->fork, 0),
               "cudaStreamWaitEvent (fork)");
@@ -791,14 +804,27 @@ int d3d_batch_autotune(d3d_batch b, void* stream) {
     for (int a : c.active) b->total_items += a;
   int rc = build_repitch(b);
   if (rc) return rc;
-  // Then the whole run with and without the cluster-resident kernel for
-  // the grids it fits (the others keep the kinds just picked).
+  // Then the whole run without the cluster-resident kernel and with it for
+  // the grids it fits in clusters of at most 4, 8, 12 or 16 CTAs (the
+  // others keep the kinds just picked): the per-step kinds are HBM-bound
+  // and the resident kernel needs SMs but next to no HBM, so a split can
+  // beat both ends.
   bool any = false;
   for (char ok : b->resident_ok) any = any || ok;
   if (!any) return D3D_OK;
-  float ms[2] = {0.0f, 0.0f};
-  for (int on = 0; on < 2; ++on) {
-    b->resident_on = on != 0;
+  static const int bounds[] = {0, 4, 8, 12, d3d::kResidentMaxCluster};
+  float times[5];
+  for (float& t : times) t = -1.0f;
+  for (int bi = 0; bi < 5; ++bi) {
+    const int bound = bounds[bi];
+    b->resident_on = bound > 0;
+    b->res_max_cluster = bound > 0 ? bound : d3d::kResidentMaxCluster;
+    if (bound > 0) {  // skip a bound that changes nothing
+      bool fresh = false;
+      for (const ResidentClass& c : b->rclasses)
+        fresh = fresh || (c.cluster <= bound && c.cluster > bound - 4);
+      if (!fresh) continue;
+    }
     rc = assign_grids(b);
     if (rc) return rc;
     rc = enqueue_all(b, s, nullptr);  // warm-up
@@ -808,9 +834,23 @@ int d3d_batch_autotune(d3d_batch b, void* stream) {
     if (rc) return rc;
     B_TRY(cudaEventRecord(b->ev[1], s), "cudaEventRecord");
     B_TRY(cudaEventSynchronize(b->ev[1]), "cudaEventSynchronize");
-    B_TRY(cudaEventElapsedTime(&ms[on], b->ev[0], b->ev[1]), "elapsed");
+    B_TRY(cudaEventElapsedTime(&times[bi], b->ev[0], b->ev[1]), "elapsed");
   }
-  b->resident_on = ms[1] < ms[0];
+  // The fastest, except that a larger bound within 2% of it wins: more
+  // grids resident means fewer launches a run (one persistent launch
+  // instead of one per step), which costs host time the device timing
+  // does not see.  (On B200 the 4096-grid batch ran 310 ms at bound 12
+  // with 1008 launches and 314 ms at 16 with 185.)
+  float best = -1.0f;
+  for (float t : times)
+    if (t >= 0.0f && (best < 0.0f || t < best)) best = t;
+  int best_bound = 0;
+  for (int bi = 0; bi < 5; ++bi)
+    if (times[bi] >= 0.0f && times[bi] <= 1.02f * best)
+      best_bound = bounds[bi];
+  b->resident_on = best_bound > 0;
+  b->res_max_cluster =
+      best_bound > 0 ? best_bound : d3d::kResidentMaxCluster;
   return assign_grids(b);
 }
 
@@ -823,6 +863,7 @@ int d3d_batch_set_kind(d3d_batch b, int kind) {
     // take the strip kind (the march kind without pitched copies).
     drop_graph(b);
     b->resident_on = true;
+    b->res_max_cluster = d3d::kResidentMaxCluster;
     for (ClassPlan& c : b->cls) c.kind = b->pitched ? kDefaultKind : 0;
     return assign_grids(b);
   }
@@ -837,6 +878,17 @@ int d3d_batch_set_kind(d3d_batch b, int kind) {
   drop_graph(b);
   b->resident_on = false;
   for (ClassPlan& c : b->cls) c.kind = kind;
+  return assign_grids(b);
+}
+
+int d3d_batch_set_resident_max_cluster(d3d_batch b, int max_cluster) {
+  if (!b) return bfail(D3D_E_INVALID, "NULL batch");
+  if (max_cluster < 0 || max_cluster > d3d::kResidentMaxCluster)
+    return bfail(D3D_E_INVALID, "max_cluster must be 0 to 16");
+  drop_graph(b);
+  b->resident_on = max_cluster > 0;
+  b->res_max_cluster =
+      max_cluster > 0 ? max_cluster : d3d::kResidentMaxCluster;
   return assign_grids(b);
 }
 
@@ -888,22 +940,25 @@ int d3d_batch_run(d3d_batch b, void* stream, float* kernel_ms) {
 int d3d_batch_info(d3d_batch b, char* buf, size_t len) {
   if (!b || !buf) return bfail(D3D_E_INVALID, "NULL argument");
   int nres = 0;
-  if (b->resident_on)
-    for (const ResidentClass& rc : b->rclasses) nres += (int)rc.grids.size();
+  for (const ResidentClass& rc : b->rclasses)
+    if (class_resident(b, rc)) nres += (int)rc.grids.size();
   int used = snprintf(buf, len,
                       "{\"grids\": %zu, \"max_steps\": %d, \"items\": %lld, "
                       "\"launches_per_run\": %llu, \"resident\": "
-                      "{\"on\": %s, \"grids\": %d, \"classes\": [",
+                      "{\"on\": %s, \"max_cluster\": %d, \"grids\": %d, "
+                      "\"classes\": [",
                       b->grids.size(), b->max_steps, b->total_items,
                       b->launches_per_run,
-                      b->resident_on ? "true" : "false", nres);
-  for (size_t ci = 0; b->resident_on && ci < b->rclasses.size() &&
-                      used < (int)len; ++ci) {
+                      b->resident_on ? "true" : "false", b->res_max_cluster,
+                      nres);
+  for (size_t ci = 0, shown = 0; ci < b->rclasses.size() && used < (int)len;
+       ++ci) {
     const ResidentClass& rc = b->rclasses[ci];
+    if (!class_resident(b, rc)) continue;
     used += snprintf(buf + used, len - used,
                      "%s{\"cluster\": %d, \"threads\": %d, \"grids\": "
                      "%zu, \"clusters\": %d, \"smem\": %zu}",
-                     ci ? ", " : "", rc.cluster,
+                     shown++ ? ", " : "", rc.cluster,
                      d3d::resident_variant(rc.variant).threads,
                      rc.grids.size(), rc.nclusters, rc.smem);
   }

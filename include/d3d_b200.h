@@ -349,10 +349,17 @@ int d3d_batch_autotune(d3d_batch batch, void* stream);
  * shared memory for all of its steps (one persistent launch per cluster
  * size and thread shape, walking its grids through a work counter); the
  * grids it does not fit take kind 4.  d3d_batch_autotune also times the
- * whole run with and without kind 8 and keeps the faster. */
+ * whole run without kind 8 and with it for the grids that fit clusters of
+ * at most 4, 8, 12 or 16 CTAs, and keeps the fastest. */
 #define D3D_BATCH_NUM_KINDS 9
 #define D3D_BATCH_KIND_RESIDENT 8
 int d3d_batch_set_kind(d3d_batch batch, int kind);
+
+/* With the cluster-resident kernel in use (kind 8 or the autotuner's
+ * pick): only grids that fit clusters of at most max_cluster CTAs
+ * (1..16) run on it, the others keep their size class's kind.
+ * max_cluster = 0 turns the resident kernel off. */
+int d3d_batch_set_resident_max_cluster(d3d_batch batch, int max_cluster);
 
 /* Per-grid step counters of the last run (n = the batch's grid count):
  * the cluster-resident kernel advances a grid's counter after each of its

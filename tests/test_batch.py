@@ -286,6 +286,40 @@ def test_cluster_resident_kind_bit_exact_with_step_counters():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("bound", [0, 1, 4, 8, 12])
+def test_cluster_resident_split_by_cluster_size(bound):
+    """Only grids that fit clusters of at most `bound` CTAs run resident
+    (0: none); the others take the strip kind in the same run.  Every grid
+    keeps the oracle's bits and reaches its step count either way."""
+    torch = pytest.importorskip("torch")
+    specs = _resident_specs(lambda i: 2 + (i * 5) % 9)
+    fields = _fields(specs, 1350)
+    batch = B.Batch(specs)
+    batch.set_kind(B.BATCH_KIND_RESIDENT)
+    every = batch.info()["resident"]["classes"]
+    batch.set_resident_max_cluster(bound)
+    for i, f in enumerate(fields):
+        batch.input(i).copy_(torch.from_numpy(f))
+    batch.run()
+    torch.cuda.synchronize()
+    for i, ((nx, ny, nz, steps, c), f) in enumerate(zip(specs, fields)):
+        assert batch.result(i).cpu().numpy().tobytes() == \
+            O.run(f, c, steps).tobytes(), (bound, nx, ny, nz)
+    assert list(batch.progress()) == [s for _, _, _, s, _ in specs]
+    res = batch.info()["resident"]
+    assert res["on"] == (bound > 0)
+    want = sum(c["grids"] for c in every if c["cluster"] <= bound)
+    assert res["grids"] == want
+    assert all(c["cluster"] <= bound for c in res["classes"])
+    for bad in (-1, 17):
+        with pytest.raises(B.D3DError) as ei:
+            batch.set_resident_max_cluster(bad)
+        assert ei.value.code == B.D3D_E_INVALID
+    assert B.check_device_errors() == 0
+    batch.close()
+
+
+@pytest.mark.gpu
 def test_cluster_resident_same_alone_and_in_the_mix():
     specs = _resident_specs(lambda i: 3 + i % 5)
     fields = _fields(specs, 1400)
