@@ -327,6 +327,20 @@ int pick_zchunk(int nz, long tiles, int ctas_per_sm, int min_chunk) {
   return (int)((nz + zs - 1) / zs);
 }
 
+// z-chunk of the TMA z-march: 12-plane chunks when they make at least four
+// waves of CTAs, else pick_zchunk's single wave.  Many short chunks keep
+// every SM busy to the end of the step; a single wave leaves the SMs it
+// does not fill idle.  Measured on B200, FP32, 32-row tiles (Gpt-updates/s,
+// one wave against 12-plane chunks): 512^3 699 / 748, 768^3 730 / 792,
+// 1024 x 1024 x 130 758 / 768; 384^3 (under four waves) 746 at one wave.
+int pick_tma_zchunk(int nz, long tiles, int ctas_per_sm) {
+  constexpr int kFine = 12;
+  const long capacity = (long)num_sms() * std::max(ctas_per_sm, 1);
+  const long ctas = tiles * ((nz + kFine - 1) / kFine);
+  if (ctas >= 4 * capacity) return kFine;
+  return pick_zchunk(nz, tiles, ctas_per_sm, 8);
+}
+
 template <typename T, int BY, int S, bool FLIP>
 cudaError_t launch_tma_t(const CUtensorMap& src, void* f2, int nx, int ny,
                          int nz, const void* coef, int zchunk_override,
@@ -350,7 +364,7 @@ cudaError_t launch_tma_t(const CUtensorMap& src, void* f2, int nx, int ny,
   const int nzr = ze - zb;
   const int zchunk = zchunk_override > 0
                          ? zchunk_override
-                         : pick_zchunk(nzr, (long)gx * gy, occ, 8);
+                         : pick_tma_zchunk(nzr, (long)gx * gy, occ);
   const int gz = (nzr + zchunk - 1) / zchunk;
   if (info) *info = LaunchInfo{gx, gy, gz, C::THREADS, C::SMEM, zchunk, occ};
   kern<<<dim3(gx, gy, gz), C::THREADS, C::SMEM, stream>>>(
@@ -385,11 +399,15 @@ int default_tma_variant(int nx, int ny, int nz, int dtype) {
   // per SM with z-chunks of 8 planes or more: at 256^3 and up that is the
   // 32-row tile (the fastest measured); small grids need shorter tiles to
   // fill the GPU (128^3: 8-row tiles, 355 against 216 Gpt/s).
+  // FP64 starts at 16 rows: its 32-row tiles measured slower on B200 at
+  // every size from 256^3 to 512^3 (512^3: 341 against 357 Gpt/s, both at
+  // 12-plane chunks).
   const long bx = 32L * (16 / (long)dtype_size(dtype));
   const long cap = 2L * num_sms();
   const long zslabs = std::max(1, nz / 8);
   const int order[3] = {0, 1, 2};  // by = 32, 16, 8
   for (int v : order) {
+    if (v == 0 && dtype_size(dtype) == 8) continue;
     const long by = kTmaVariants[v].by;
     const long tiles = ((nx + bx - 1) / bx) * ((ny + by - 1) / by) * zslabs;
     if (tiles >= cap) return v;

@@ -319,13 +319,18 @@ cudaError_t launch_tb2w_t(const CUtensorMap& src, void* f2, int nx, int ny,
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int gx = (nx + C::BX - 1) / C::BX;
   const int gy = (ny + C::BY - 1) / C::BY;
-  (void)sms;
   int zchunk = zchunk_override;
   if (zchunk <= 0) {
     // Measured on B200 (Gpt-updates/s): 96-plane chunks at 512^3 (826-837)
     // and 768^3 (849); shorter grids need more chunks to keep CTAs in
     // flight (384^3: 32 planes, 743 against 573-695 for 48-128; 256^3: 16).
-    zchunk = std::min(nz, nz >= 512 ? 96 : nz >= 384 ? 32 : 16);
+    // Shallow grids of wide planes, whose tiles alone fill two waves, take
+    // 128-plane chunks instead of short ones (a z slab of a 1024^2 grid,
+    // 130 planes: 840 at 128 against 751 at 16).
+    if (nz < 512 && (long)gx * gy >= 2L * sms * std::max(occ, 1))
+      zchunk = std::min(nz, 128);
+    else
+      zchunk = std::min(nz, nz >= 512 ? 96 : nz >= 384 ? 32 : 16);
   }
   const int gz = (nz + zchunk - 1) / zchunk;
   if (info) *info = LaunchInfo{gx, gy, gz, C::THREADS, C::SMEM, zchunk, occ};
