@@ -247,6 +247,28 @@ def test_full_size_512_kernels_agree():
     assert B.check_device_errors() == 0
 
 
+@pytest.mark.parametrize("dims,dtype", [((1024, 1024, 61), np.float32),
+                                        ((1024, 512, 61), np.float64)])
+def test_fine_zchunks_on_wide_grids_vs_oracle(dims, dtype):
+    """Grids wide enough that the TMA z-march cuts 12-plane chunks (four
+    or more waves of CTAs): nz = 61 leaves a last chunk of one plane.  The
+    automatic launch shape is checked, then the bits against the oracle."""
+    nx, ny, nz = dims
+    c, _ = O.params(nx, ny, nz, dtype)
+    fin = O.seeded_noise((nz, ny, nx), 61, amplitude=1.0).astype(dtype)
+    plan = B.Plan(nx, ny, nz, B.F64 if dtype == np.float64 else B.F32,
+                  B.KERNEL_TMA)
+    f1 = torch.from_numpy(fin).cuda()
+    f2 = torch.empty_like(f1)
+    res, _ = plan.run(f1, f2, 3, c)
+    torch.cuda.synchronize()
+    info = plan.info()
+    assert info["launch_zchunk"] == 12, info
+    assert B.check_device_errors() == 0
+    assert bits_equal(res.cpu().numpy(), O.run(fin, c, 3))
+    plan.close()
+
+
 def test_device_compare_matches_oracle_norms():
     a = O.seeded_noise((40, 30, 20), 1, amplitude=1.0) + np.float32(0.5)
     b = a + O.seeded_noise(a.shape, 2, amplitude=1e-3)
