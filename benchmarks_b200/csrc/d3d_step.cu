@@ -476,7 +476,16 @@ cudaError_t launch_step_generic(const void* f1, void* f2, int nx, int ny,
   const int by = dtype == kF64 ? GenTile<double>::BY : GenTile<float>::BY;
   const int gx = (nx + bx - 1) / bx;
   const int gy = (ny + by - 1) / by;
-  const int zchunk = pick_zchunk(ze - zb, (long)gx * gy, 8, 32);
+  // 24-plane chunks when they make four or more waves (8 CTAs an SM),
+  // else one wave of chunks of 32 planes or more.  Measured on B200
+  // (Gpt-updates/s, one wave against 24-plane chunks): FP32 511^3 551 /
+  // 622, 767^3 566 / 618; FP64 511^3 290 / 354.
+  constexpr int kFine = 24;
+  const long tiles = (long)gx * gy;
+  const int zchunk =
+      tiles * ((ze - zb + kFine - 1) / kFine) >= 4L * num_sms() * 8
+          ? kFine
+          : pick_zchunk(ze - zb, tiles, 8, 32);
   const int gz = (ze - zb + zchunk - 1) / zchunk;
   if (info) *info = LaunchInfo{gx, gy, gz, 256, 0, zchunk, 8};
   dim3 grid(gx, gy, gz), block(256);
