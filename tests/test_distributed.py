@@ -303,3 +303,108 @@ def test_slab_transport_failure_is_reported():
         torch.cuda.synchronize()
     finally:
         B.lib().d3d_slab_destroy(slab)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("world,halo,dims,count", [
+    (2, 2, (128, 40, 36), 9),
+    (3, 3, (96, 24, 40), 7),
+    (4, 2, (64, 17, 33), 10),
+])
+def test_slab_runner_threads_exchange_device_planes(world, halo, dims,
+                                                    count):
+    """d3d_slab_run with a transport of the caller's own: each rank is a
+    host thread with its own stream and slab, and the planes move device to
+    device (no torch.distributed, no host staging).  Waits are host-side and
+    bounded (a barrier with a timeout); no kernel waits on another rank's.
+    The owned planes gathered from all ranks equal the oracle's run."""
+    import ctypes
+    import threading
+
+    import benchmarks_b200 as B
+    import oracle as O
+    import torch
+    from benchmarks_b200.distributed import SlabDecomposition, _SlabTransport
+
+    nx, ny, nz = dims
+    c, _ = O.params(nx, ny, nz)
+    field = O.initialize(nx, ny, nz) + O.seeded_noise((nz, ny, nx), 9)
+    g = torch.from_numpy(field).cuda()
+    decs = [SlabDecomposition(nz, r, world, halo) for r in range(world)]
+    posted = [None] * world           # this pass's (send, recv) per rank
+    barrier = threading.Barrier(world, timeout=60)
+    errors = [None] * world
+    results = [None] * world
+
+    def rank_main(r):
+        d = decs[r]
+        stream = torch.cuda.Stream()
+        slab = ctypes.c_void_p()
+        lnz = ctypes.c_int()
+        try:
+            B.check(B.lib().d3d_slab_create(nx, ny, nz, d.z0, d.z1, halo,
+                                            B.F32, ctypes.byref(slab),
+                                            ctypes.byref(lnz)))
+            assert lnz.value == d.local_nz
+            f1 = g[d.lo:d.hi].clone()
+            f2 = torch.empty_like(f1)
+            torch.cuda.synchronize()
+
+            def post(user, send, recv, nbytes, s):
+                try:  # the planes to send are ready once this stream is
+                    B.check(B.lib().d3d_stream_sync(s))
+                except Exception as e:
+                    errors[r] = e
+                    barrier.abort()
+                    return 1
+                posted[r] = ([send[0], send[1]], [recv[0], recv[1]], nbytes)
+                return 0
+
+            def wait(user, s):
+                try:
+                    barrier.wait()           # every rank has posted
+                    _, recv, nbytes = posted[r]
+                    for side, peer, their in ((0, r - 1, 1), (1, r + 1, 0)):
+                        if recv[side]:
+                            B.check(B.lib().d3d_memcpy(
+                                recv[side], posted[peer][0][their], nbytes,
+                                s))
+                    B.check(B.lib().d3d_stream_sync(s))
+                    barrier.wait()           # every rank has copied
+                    return 0
+                except Exception as e:  # reported as a transport failure
+                    errors[r] = e
+                    barrier.abort()
+                    return 1
+
+            keep = (_SlabTransport.POST(post), _SlabTransport.WAIT(wait))
+            t = _SlabTransport.Struct(
+                ctypes.cast(keep[0], ctypes.c_void_p),
+                ctypes.cast(keep[1], ctypes.c_void_p), None)
+            a = ctypes.c_void_p(f1.data_ptr())
+            b = ctypes.c_void_p(f2.data_ptr())
+            B.check(B.lib().d3d_slab_run(slab, ctypes.byref(a),
+                                         ctypes.byref(b), c.ctypes.data,
+                                         count, ctypes.byref(t),
+                                         stream.cuda_stream))
+            torch.cuda.synchronize()
+            res = f1 if a.value == f1.data_ptr() else f2
+            results[r] = res[d.owned()].cpu().numpy()
+        except Exception as e:
+            if errors[r] is None:
+                errors[r] = e
+            barrier.abort()
+        finally:
+            B.lib().d3d_slab_destroy(slab)
+
+    threads = [threading.Thread(target=rank_main, args=(r,))
+               for r in range(world)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join(timeout=300)
+    assert not any(th.is_alive() for th in threads)
+    assert errors == [None] * world, errors
+    full = np.concatenate(results)
+    assert full.tobytes() == O.run(field, c, count).tobytes()
+    assert B.check_device_errors() == 0
