@@ -726,8 +726,15 @@ def run_b200(args):
         "side": side,
     }
     if not args.no_side:
-        # Every rank takes part (the exchange is a collective step).
-        side["slab"] = slab_leg(B, torch, dist)
+        # Every rank takes part (the exchange is a collective step).  A
+        # failure here is recorded in the line rather than losing the
+        # headline measured above; the process group's timeout bounds a
+        # rank left waiting for a failed peer.
+        try:
+            side["slab"] = slab_leg(B, torch, dist)
+        except Exception as e:  # noqa: BLE001 -- reported, not hidden
+            side["slab"] = {"error": "%s: %s" % (type(e).__name__, e)}
+            torch.cuda.synchronize()
     if not args.no_side and world == 1:
         del a, b, f1, f2, host, init
         torch.cuda.empty_cache()
