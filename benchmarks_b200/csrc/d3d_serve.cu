@@ -219,6 +219,63 @@ int sfail(int code, const char* msg) { return d3d::set_error(code, "%s", msg); }
     if (e__ != cudaSuccess) return d3d::set_cuda_error(e__, what);    \
   } while (0)
 
+void free_res_staging(ResStaging* st) {
+  if (st->h) cudaFreeHost(st->h);
+  if (st->d) cudaFree(st->d);
+  if (st->d_steps) cudaFree(st->d_steps);
+  if (st->d_queue) cudaFree(st->d_queue);
+  if (st->done) cudaEventDestroy(st->done);
+  if (st->stream) cudaStreamDestroy(st->stream);
+  delete st;
+}
+
+// The resident path's stream pool, events and staging ring.  Streams and
+// events missing after an earlier failure are made now; the ring is made
+// whole or not at all, so a failed call leaves no half-built staging.
+int make_resident_state(d3d_server s) {
+  for (int i = 0; i < kResStreams; ++i) {
+    if (!s->res_pool[i])
+      S_TRY(cudaStreamCreateWithFlags(&s->res_pool[i],
+                                      cudaStreamNonBlocking),
+            "cudaStreamCreate");
+    if (!s->res_join[i])
+      S_TRY(cudaEventCreateWithFlags(&s->res_join[i],
+                                     cudaEventDisableTiming),
+            "cudaEventCreate");
+  }
+  if (!s->res_ready)
+    S_TRY(cudaEventCreateWithFlags(&s->res_ready, cudaEventDisableTiming),
+          "cudaEventCreate");
+  if (!s->rstage.empty()) return D3D_OK;
+  std::vector<ResStaging*> ring;
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < kResStages && e == cudaSuccess; ++i) {
+    ResStaging* st = new (std::nothrow) ResStaging();
+    if (!st) {
+      for (ResStaging* r : ring) free_res_staging(r);
+      return sfail(D3D_E_OOM, "resident staging");
+    }
+    ring.push_back(st);
+    st->cap = kResGroupCap;
+    e = cudaMallocHost(&st->h, st->cap * sizeof(d3d::ResidentDesc));
+    if (e == cudaSuccess)
+      e = cudaMalloc(&st->d, st->cap * sizeof(d3d::ResidentDesc));
+    if (e == cudaSuccess) e = cudaMalloc(&st->d_steps, st->cap * sizeof(int));
+    if (e == cudaSuccess)
+      e = cudaMalloc(&st->d_queue, kMaxResClasses * sizeof(unsigned));
+    if (e == cudaSuccess)
+      e = cudaEventCreateWithFlags(&st->done, cudaEventDisableTiming);
+    if (e == cudaSuccess)
+      e = cudaStreamCreateWithFlags(&st->stream, cudaStreamNonBlocking);
+  }
+  if (e != cudaSuccess) {
+    for (ResStaging* r : ring) free_res_staging(r);
+    return d3d::set_cuda_error(e, "resident staging");
+  }
+  s->rstage.swap(ring);
+  return D3D_OK;
+}
+
 int ensure_staging(Staging& st, size_t desc_bytes, size_t nitems) {
   if (desc_bytes > st.cap_desc) {
     if (st.h_desc) cudaFreeHost(st.h_desc);
@@ -882,37 +939,9 @@ int d3d_server_set_resident(d3d_server s, int on) {
       !s->res_pending.empty())
     return sfail(D3D_E_BUSY,
                  "the resident path changes only on an idle server");
-  if (on && !s->res_ready) {
-    for (int i = 0; i < kResStreams; ++i) {
-      S_TRY(cudaStreamCreateWithFlags(&s->res_pool[i],
-                                      cudaStreamNonBlocking),
-            "cudaStreamCreate");
-      S_TRY(cudaEventCreateWithFlags(&s->res_join[i],
-                                     cudaEventDisableTiming),
-            "cudaEventCreate");
-    }
-    S_TRY(cudaEventCreateWithFlags(&s->res_ready, cudaEventDisableTiming),
-          "cudaEventCreate");
-  }
-  if (on && s->rstage.empty()) {
-    for (int i = 0; i < kResStages; ++i) {
-      ResStaging* st = new (std::nothrow) ResStaging();
-      if (!st) return sfail(D3D_E_OOM, "resident staging");
-      s->rstage.push_back(st);  // freed by d3d_server_destroy
-      st->cap = kResGroupCap;
-      S_TRY(cudaMallocHost(&st->h, st->cap * sizeof(d3d::ResidentDesc)),
-            "cudaMallocHost (resident staging)");
-      S_TRY(cudaMalloc(&st->d, st->cap * sizeof(d3d::ResidentDesc)),
-            "cudaMalloc (resident staging)");
-      S_TRY(cudaMalloc(&st->d_steps, st->cap * sizeof(int)),
-            "cudaMalloc (resident step counters)");
-      S_TRY(cudaMalloc(&st->d_queue, kMaxResClasses * sizeof(unsigned)),
-            "cudaMalloc (resident work counters)");
-      S_TRY(cudaEventCreateWithFlags(&st->done, cudaEventDisableTiming),
-            "cudaEventCreate");
-      S_TRY(cudaStreamCreateWithFlags(&st->stream, cudaStreamNonBlocking),
-            "cudaStreamCreate");
-    }
+  if (on) {
+    const int rc = make_resident_state(s);
+    if (rc) return rc;
   }
   s->resident = on != 0;
   return D3D_OK;
@@ -992,15 +1021,7 @@ int d3d_server_destroy(d3d_server s) {
   for (Request* r : s->active) free_request(s, r);
   for (Request* r : s->res_pending) free_request(s, r);
   for (Request* r : s->retiring) free_request(s, r);
-  for (ResStaging* st : s->rstage) {
-    if (st->h) cudaFreeHost(st->h);
-    if (st->d) cudaFree(st->d);
-    if (st->d_steps) cudaFree(st->d_steps);
-    if (st->d_queue) cudaFree(st->d_queue);
-    if (st->done) cudaEventDestroy(st->done);
-    if (st->stream) cudaStreamDestroy(st->stream);
-    delete st;
-  }
+  for (ResStaging* st : s->rstage) free_res_staging(st);
   for (int i = 0; i < kResStreams; ++i) {
     if (s->res_pool[i]) cudaStreamDestroy(s->res_pool[i]);
     if (s->res_join[i]) cudaEventDestroy(s->res_join[i]);
