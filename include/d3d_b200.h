@@ -448,8 +448,11 @@ int d3d_server_set_large_kernel(d3d_server server, int kernel, int min_px);
  * within one cluster's shared memory, the rule of D3D_BATCH_KIND_RESIDENT)
  * takes one dense buffer of the arena instead of two, and all of its steps
  * run in one persistent launch per cluster size together with the other
- * such solves admitted in the same tick; the ticks' step launches carry
- * only the larger solves. */
+ * such solves admitted in the same tick, each launch on an idle stream of
+ * a pool of 16; the ticks' step launches carry only the larger solves.
+ * The first switch to on allocates the path's streams and its ring of 16
+ * group stagings (pinned and device, 256 solves each), so serving itself
+ * allocates nothing; on failure nothing of the ring is kept. */
 int d3d_server_set_resident(d3d_server server, int on);
 
 /* Number of requests queued, active on the device and copying out. */
