@@ -327,17 +327,19 @@ int pick_zchunk(int nz, long tiles, int ctas_per_sm, int min_chunk) {
   return (int)((nz + zs - 1) / zs);
 }
 
-// z-chunk of the TMA z-march: 12-plane chunks when they make at least four
-// waves of CTAs, else pick_zchunk's single wave.  Many short chunks keep
-// every SM busy to the end of the step; a single wave leaves the SMs it
-// does not fill idle.  Measured on B200, FP32, 32-row tiles (Gpt-updates/s,
-// one wave against 12-plane chunks): 512^3 699 / 748, 768^3 730 / 792,
-// 1024 x 1024 x 130 758 / 768; 384^3 (under four waves) 746 at one wave.
-int pick_tma_zchunk(int nz, long tiles, int ctas_per_sm) {
-  constexpr int kFine = 12;
+// z-chunk of the TMA z-march: short chunks (16 planes FP32, 12 FP64) when
+// they make at least four waves of CTAs, else pick_zchunk's single wave.
+// Many short chunks keep every SM busy to the end of the step; a single
+// wave leaves the SMs it does not fill idle.  Measured on B200
+// (Gpt-updates/s, one wave against short chunks, short runs): FP32 768^3
+// 706-731 / 769-795, 1024 x 1024 x 130 758 / 757-768; FP64 512^3 303-315 /
+// 347-357.  At 512^3 FP32, sustained over 0.8 s under the power cap, one
+// wave and 16-plane chunks tie (720.1 / 719.5, five alternating rounds)
+// while 12-plane chunks draw more power and run 1% slower (712.9).
+int pick_tma_zchunk(int nz, long tiles, int ctas_per_sm, int fine) {
   const long capacity = (long)num_sms() * std::max(ctas_per_sm, 1);
-  const long ctas = tiles * ((nz + kFine - 1) / kFine);
-  if (ctas >= 4 * capacity) return kFine;
+  const long ctas = tiles * ((nz + fine - 1) / fine);
+  if (ctas >= 4 * capacity) return fine;
   return pick_zchunk(nz, tiles, ctas_per_sm, 8);
 }
 
@@ -364,7 +366,8 @@ cudaError_t launch_tma_t(const CUtensorMap& src, void* f2, int nx, int ny,
   const int nzr = ze - zb;
   const int zchunk = zchunk_override > 0
                          ? zchunk_override
-                         : pick_tma_zchunk(nzr, (long)gx * gy, occ);
+                         : pick_tma_zchunk(nzr, (long)gx * gy, occ,
+                                           sizeof(T) == 8 ? 12 : 16);
   const int gz = (nzr + zchunk - 1) / zchunk;
   if (info) *info = LaunchInfo{gx, gy, gz, C::THREADS, C::SMEM, zchunk, occ};
   kern<<<dim3(gx, gy, gz), C::THREADS, C::SMEM, stream>>>(

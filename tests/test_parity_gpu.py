@@ -247,12 +247,13 @@ def test_full_size_512_kernels_agree():
     assert B.check_device_errors() == 0
 
 
-@pytest.mark.parametrize("dims,dtype", [((1024, 1024, 61), np.float32),
-                                        ((1024, 512, 61), np.float64)])
-def test_fine_zchunks_on_wide_grids_vs_oracle(dims, dtype):
-    """Grids wide enough that the TMA z-march cuts 12-plane chunks (four
-    or more waves of CTAs): nz = 61 leaves a last chunk of one plane.  The
-    automatic launch shape is checked, then the bits against the oracle."""
+@pytest.mark.parametrize("dims,dtype,fine", [
+    ((1024, 1024, 65), np.float32, 16), ((1024, 512, 61), np.float64, 12)])
+def test_fine_zchunks_on_wide_grids_vs_oracle(dims, dtype, fine):
+    """Grids wide enough that the TMA z-march cuts short chunks (16 planes
+    FP32, 12 FP64; four or more waves of CTAs): nz leaves a last chunk of
+    one plane.  The automatic launch shape is checked, then the bits
+    against the oracle."""
     nx, ny, nz = dims
     c, _ = O.params(nx, ny, nz, dtype)
     fin = O.seeded_noise((nz, ny, nx), 61, amplitude=1.0).astype(dtype)
@@ -263,7 +264,7 @@ def test_fine_zchunks_on_wide_grids_vs_oracle(dims, dtype):
     res, _ = plan.run(f1, f2, 3, c)
     torch.cuda.synchronize()
     info = plan.info()
-    assert info["launch_zchunk"] == 12, info
+    assert info["launch_zchunk"] == fine, info
     assert B.check_device_errors() == 0
     assert bits_equal(res.cpu().numpy(), O.run(fin, c, 3))
     plan.close()
