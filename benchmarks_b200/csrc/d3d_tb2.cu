@@ -321,12 +321,31 @@ cudaError_t launch_tb2w_t(const CUtensorMap& src, void* f2, int nx, int ny,
   const int gy = (ny + C::BY - 1) / C::BY;
   int zchunk = zchunk_override;
   if (zchunk <= 0) {
-    // Measured on B200 (Gpt-updates/s): 96-plane chunks at 512^3 (826-837)
-    // and 768^3 (849); shorter grids need more chunks to keep CTAs in
-    // flight (384^3: 32 planes, 743 against 573-695 for 48-128; 256^3: 16).
-    // Shallow grids of wide planes, whose tiles alone fill two waves, take
-    // 128-plane chunks instead of short ones (a z slab of a 1024^2 grid,
-    // 130 planes: 840 at 128 against 751 at 16).
+    // The longest chunk of 256, 128 or 96 planes whose CTAs fill at least
+    // one wave and leave the last wave empty or at least 90% full: longer
+    // chunks recompute fewer halo planes, a part-filled last wave idles
+    // SMs.  Sustained on B200 (Gpt-updates/s): 512^3 (whole waves at all
+    // three) 842.5 / 839.7 / 825.9 at 256 / 128 / 96; 768^3 851 at 96
+    // (last wave 92% full) against 828 at 128 and 802 at 256; 1024^3 858 at
+    // 256.
+    const long cap = (long)sms * std::max(occ, 1);
+    const long tiles = (long)gx * gy;
+    for (int z : {256, 128, 96}) {
+      const long ctas = tiles * ((nz + z - 1) / z);
+      const long rem = ctas % cap;
+      if (ctas >= cap && (rem == 0 || rem * 10 >= cap * 9)) {
+        zchunk = std::min(nz, z);
+        break;
+      }
+    }
+  }
+  if (zchunk <= 0) {
+    // Otherwise (measured on B200): 96 planes from nz = 512 on, 32 at
+    // 384^3 (743 against 573-695 for 48-128), 16 for shorter grids, which
+    // need more chunks to keep CTAs in flight.  Shallow grids of wide
+    // planes, whose tiles alone fill two waves, take 128-plane chunks
+    // instead of short ones (a z slab of a 1024^2 grid, 130 planes: 840 at
+    // 128 against 751 at 16).
     if (nz < 512 && (long)gx * gy >= 2L * sms * std::max(occ, 1))
       zchunk = std::min(nz, 128);
     else
